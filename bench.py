@@ -1,0 +1,426 @@
+"""Benchmark: the radar front end + range-Doppler chain at scale on B200.
+
+Workload (one step = one CPI):
+  front end  16 channels x 2^20 float32 -> 127-tap Kaiser(8) lowpass firfilter ->
+             resample_poly 3/2 (default Kaiser(5), 61 taps) -> 16 x 1572864 float32
+  chain      1024 pulses x 16384 range complex64 CPI (64 targets, 1024-sample LFM
+             chirp) -> pulse_compression (Hamming replica, normalised) ->
+             pulse_doppler (Hamming over pulses) + |.|^2 -> 2-D CA-CFAR
+             (guard 2x2, train 8x8, Pfa 1e-6)
+Inputs are seeded synthetic data; each timed step reads a different input set (three
+rotating sets, every set larger than the 126 MB L2), so no step starts with its inputs
+cached.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (torchrun, one rank per GPU) runs independent replicas: CPIs are independent,
+there is no data exchange; the barrier and the max-over-ranks time are the only
+collectives.  Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "CPIs/sec + HBM GB/s, range-Doppler+CFAR; p99 latency; rel err vs FP64"
+UNIT = "CPIs/s"
+WORKLOAD = "front end 16x2^20 fir127+resample_poly 3/2 + range-Doppler-CFAR 1024x16384"
+
+P, NR, L = 1024, 16384, 1024
+CH, NS = 16, 1 << 20
+FIR_TAPS, FIR_BETA, FIR_CUTOFF = 127, 8.0, 0.3
+UP, DOWN = 3, 2
+N_TARGETS = 64
+CELLS = P * NR
+
+# algorithmic bytes per launch (compulsory reads + writes)
+ALG_BYTES = {
+    "fir": CH * NS * 8,
+    "resample_poly": CH * NS * 4 + CH * (NS * UP // DOWN) * 4,
+    "pulse_compression": CELLS * 16,
+    "pulse_doppler": CELLS * 20,
+    "ca_cfar": CELLS * 9,
+}
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic():
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------- our arm
+
+def run_ours(args, rank: int, world: int, dist) -> dict:
+    import torch
+    import zkx_dev_b200 as z
+    from zkx_dev_b200 import synth
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+
+    # inputs: three rotating sets (host pinned + device copies)
+    n_sets = 3
+    host_fe, host_cube = [], []
+    for i in range(n_sets):
+        seed = synth.seed_for(2, rank * 100 + i)
+        host_fe.append(torch.from_numpy(synth.make_front_end(CH, NS, seed)).pin_memory())
+        cpi = synth.make_cpi(P, NR, N_TARGETS, L, seed)
+        host_cube.append(torch.from_numpy(cpi.x).pin_memory())
+        replica = cpi.replica
+    dev_fe = [h.to(dev) for h in host_fe]
+    dev_cube = [h.to(dev) for h in host_cube]
+
+    taps_fir = torch.as_tensor(synth.firwin_kaiser(FIR_TAPS, FIR_CUTOFF, FIR_BETA).astype(np.float32), device=dev)
+    taps_rs = torch.as_tensor(z.resample_poly_taps(NS, UP, DOWN, 5.0).astype(np.float32), device=dev)
+    chain = z.RangeDopplerChain(z.ChainConfig(P, NR, L, pfa=1e-6), torch.as_tensor(replica, device=dev))
+    out = chain.allocate_outputs()
+    fir_out = torch.empty((CH, NS), dtype=torch.float32, device=dev)
+    from zkx_dev_b200 import _lib as LB
+    import ctypes
+    lay = z.filtering.resample_layout(NS, UP, DOWN)
+    rs_out = torch.empty((CH, lay.output_samples), dtype=torch.float32, device=dev)
+    lib = LB.lib()
+    sh = LB.stream_handle()
+
+    def front_end(x):
+        LB.check(lib.zkx_fir_f32(taps_fir.data_ptr(), FIR_TAPS, x.data_ptr(), CH, NS, None,
+                                 fir_out.data_ptr(), None, sh))
+        LB.check(lib.zkx_resample_poly_f32(fir_out.data_ptr(), CH, NS, ctypes.byref(lay),
+                                           taps_rs.data_ptr(), rs_out.data_ptr(), sh))
+
+    def step(i, events=None):
+        k = i % n_sets
+        if events is not None:
+            events[0].record(stream)
+        LB.check(lib.zkx_fir_f32(taps_fir.data_ptr(), FIR_TAPS, dev_fe[k].data_ptr(), CH, NS, None,
+                                 fir_out.data_ptr(), None, sh))
+        if events is not None:
+            events[1].record(stream)
+        LB.check(lib.zkx_resample_poly_f32(fir_out.data_ptr(), CH, NS, ctypes.byref(lay),
+                                           taps_rs.data_ptr(), rs_out.data_ptr(), sh))
+        if events is not None:
+            events[2].record(stream)
+        chain(dev_cube[k], out)
+        if events is not None:
+            events[3].record(stream)
+
+    # warm-up
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+
+    # per-stage timing (separate pass, kernels bracketed by events)
+    stage_ms = {k: [] for k in ("fir", "resample_poly", "pulse_compression", "pulse_doppler", "ca_cfar")}
+    for i in range(max(3, args.steps)):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+        k = i % n_sets
+        ev[0].record(stream)
+        LB.check(lib.zkx_fir_f32(taps_fir.data_ptr(), FIR_TAPS, dev_fe[k].data_ptr(), CH, NS, None,
+                                 fir_out.data_ptr(), None, sh))
+        ev[1].record(stream)
+        LB.check(lib.zkx_resample_poly_f32(fir_out.data_ptr(), CH, NS, ctypes.byref(lay),
+                                           taps_rs.data_ptr(), rs_out.data_ptr(), sh))
+        ev[2].record(stream)
+        LB.check(lib.zkx_pulse_compression_spectrum_c64(dev_cube[k].data_ptr(), P, NR, NR,
+                                                        chain_spectrum(chain), out["compressed"].data_ptr(), sh))
+        ev[3].record(stream)
+        LB.check(lib.zkx_pulse_doppler_c64(out["compressed"].data_ptr(), P, NR, P, LB.WINDOW_HAMMING, None,
+                                           out["rd"].data_ptr(), out["power"].data_ptr(), sh))
+        ev[4].record(stream)
+        LB.check(lib.zkx_ca_cfar_f32(out["power"].data_ptr(), 2, P, NR, 2, 2, 8, 8, 1e-6, LB.CFAR_ACCURATE,
+                                     out["threshold"].data_ptr(), out["detections"].data_ptr(), sh))
+        ev[5].record(stream)
+        torch.cuda.synchronize()
+        for j, name in enumerate(stage_ms):
+            stage_ms[name].append(ev[j].elapsed_time(ev[j + 1]))
+
+    # timed region: K steps, device time, max over ranks
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for i in range(args.steps):
+        step(i)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    elapsed_ms = t0.elapsed_time(t1)
+
+    # end to end through the public API with host buffers: H2D inputs, compute, D2H result
+    host_det = torch.empty((P, NR), dtype=torch.uint8).pin_memory()
+    h2d = CH * NS * 4 + CELLS * 8
+    d2h = CELLS
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    xin_fe = torch.empty((CH, NS), dtype=torch.float32, device=dev)
+    xin_cube = torch.empty((P, NR), dtype=torch.complex64, device=dev)
+    for i in range(2):
+        xin_fe.copy_(host_fe[i % n_sets], non_blocking=True)
+        xin_cube.copy_(host_cube[i % n_sets], non_blocking=True)
+        front_end(xin_fe)
+        chain(xin_cube, out)
+        host_det.copy_(out["detections"], non_blocking=True)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0.record(stream)
+    for i in range(args.steps):
+        xin_fe.copy_(host_fe[i % n_sets], non_blocking=True)
+        xin_cube.copy_(host_cube[i % n_sets], non_blocking=True)
+        front_end(xin_fe)
+        chain(xin_cube, out)
+        host_det.copy_(out["detections"], non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+
+    if dist is not None:
+        import torch.distributed as tdist
+        t = torch.tensor([elapsed_ms, e2e_ms], device=dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        elapsed_ms, e2e_ms = float(t[0]), float(t[1])
+
+    chain.close()
+    per_stage = {k: statistics.median(v) for k, v in stage_ms.items()}
+    dominant = max(per_stage, key=per_stage.get)
+    peak, peak_kind = _peaks()
+    achieved = ALG_BYTES[dominant] / (per_stage[dominant] * 1e-3) / 1e9
+    traffic = _traffic().get(dominant)
+    stage_gbs = {k: round(ALG_BYTES[k] / (v * 1e-3) / 1e9, 1) for k, v in per_stage.items()}
+    return {
+        "value": world * args.steps / (elapsed_ms * 1e-3),
+        "ms_per_step": elapsed_ms / args.steps,
+        "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1),
+                     "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic},
+        "stages_ms": {k: round(v, 4) for k, v in per_stage.items()},
+        "stages_gbs": stage_gbs,
+        "chain_gbs": round(sum(ALG_BYTES.values()) / (elapsed_ms / args.steps * 1e-3) / 1e9, 1),
+        "gpu_launches": 5 * args.steps,
+        "clocks": clk,
+    }
+
+
+def chain_spectrum(chain) -> int:
+    """Device pointer of a plan's resident replica spectrum, via a fresh spectrum call
+    with the plan's settings (kept alive on the chain object)."""
+    import zkx_dev_b200 as z
+    if not hasattr(chain, "_bench_spectrum"):
+        chain._bench_spectrum = z.replica_spectrum(chain._keep[0], chain.range_bins, normalize=True,
+                                                   window="hamming")
+    return chain._bench_spectrum.data_ptr()
+
+
+# ---------------------------------------------------------------- reference arm
+
+def reference_cpu_baseline(steps: int, warmup: int) -> dict:
+    """The reference's own CPU implementation (oracle/_ref: *_typed_cpu<float>) on a
+    bounded sample of the same workload, all host threads, scaled to CPIs/s."""
+    import concurrent.futures as cf
+    import oracle as O
+    from zkx_dev_b200 import synth
+
+    if O.reference() is None:
+        impl, kind = "port", "port"
+    else:
+        impl, kind = "reference", "reference"
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    rng_seed = synth.seed_for(2, 999)
+    cpi = synth.make_cpi(P, NR, N_TARGETS, L, rng_seed)
+    fe = synth.make_front_end(1, 1 << 16, rng_seed)[0]
+    fir_taps = synth.firwin_kaiser(FIR_TAPS, FIR_CUTOFF, FIR_BETA).astype(np.float32)
+    w_r = O.radar_window_f32("hamming", L)
+    # samples (fraction of one CPI's work each)
+    samples = {
+        "fir": (lambda: (O.ref_firfilter if impl == "reference" else O.firfilter)(fir_taps, fe[None, :]),
+                (1 << 16) / (CH * NS)),
+        "resample_poly": (lambda: (O.ref_resample_poly(fe[None, :], UP, DOWN) if impl == "reference"
+                                   else O.resample_poly(fe[None, :], UP, DOWN)), (1 << 16) / (CH * NS)),
+        "pulse_compression": (lambda: (O.ref_pulse_compression(cpi.x[:1], cpi.replica, -1, True, "hamming")
+                                       if impl == "reference" else
+                                       O.pulse_compression_direct(cpi.x[:1], cpi.replica, -1, True, "hamming")),
+                              1.0 / P),
+        "pulse_doppler": (lambda: (O.ref_pulse_doppler(cpi.x[:, :4], -1, "hamming") if impl == "reference"
+                                   else O.pulse_doppler_direct(cpi.x[:, :4], -1, "hamming")), 4.0 / NR),
+        "ca_cfar": (lambda: (O.ref_ca_cfar if impl == "reference" else O.ca_cfar_compat)(
+            np.abs(cpi.x[:, :1024]) ** 2, (2, 2), (8, 8), 1e-6), 1024.0 / NR),
+    }
+    per_cpi_s = []
+    stage_s = {}
+    with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+        for it in range(warmup + steps):
+            total = 0.0
+            for name, (fn, frac) in samples.items():
+                t0 = time.perf_counter()
+                list(ex.map(lambda _: fn(), range(cores)))
+                wall = time.perf_counter() - t0
+                # cores samples ran concurrently: one CPI of this stage takes wall/(cores*frac)
+                cpi_s = wall / (cores * frac)
+                total += cpi_s
+                if it >= warmup:
+                    stage_s.setdefault(name, []).append(cpi_s)
+            if it >= warmup:
+                per_cpi_s.append(total)
+    t = statistics.median(per_cpi_s)
+    return {"value": 1.0 / t, "unit": UNIT, "cores": cores, "kind": kind,
+            "seconds_per_cpi": t,
+            "stage_seconds_per_cpi": {k: statistics.median(v) for k, v in stage_s.items()},
+            "sample": ("per stage and thread: firfilter + resample_poly on 2^16 samples of one "
+                       "channel, pulse_compression of 1 pulse, pulse_doppler of 4 range columns "
+                       "x 1024 pulses, ca_cfar on 1024x1024; scaled by the sampled fraction of "
+                       "one 1024x16384 CPI + 16x2^20 front end")}
+
+
+# ------------------------------------------------------------------------ main
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    config = {"workload": WORKLOAD, "pulses": P, "range": NR, "chirp": L, "targets": N_TARGETS,
+              "front_end": f"{CH}x{NS} fir{FIR_TAPS} resample {UP}/{DOWN}",
+              "cfar": "guard 2x2 train 8x8 pfa 1e-6", "parallelism": f"replicas{world}",
+              "l2": "inputs larger than L2, three rotating input sets"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        base = reference_cpu_baseline(max(1, min(args.steps, 3)), 1)
+        line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / base["value"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded CN(0,1) + LFM targets)", "config": config,
+                "impl": "reference",
+                "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "stage_seconds_per_cpi": base["stage_seconds_per_cpi"]}
+        print(json.dumps(line))
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    res = run_ours(args, rank, world, dist)
+    if rank == 0:
+        line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded CN(0,1) + LFM targets)", "config": config,
+                "e2e": res["e2e"], "roofline": res["roofline"], "gpu_launches": res["gpu_launches"],
+                "clocks": res["clocks"], "stages_ms": res["stages_ms"], "stages_gbs": res["stages_gbs"],
+                "chain_gbs": res["chain_gbs"]}
+        if world == 1 and not args.no_cpu_baseline:
+            base = reference_cpu_baseline(1, 0)
+            line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,218 @@
+/*
+ * zkx_rd.h -- C ABI of the B200 radar range-Doppler library (libzkx_rd.so).
+ *
+ * Every entry point takes plain device pointers, element counts and a CUDA stream,
+ * returns an int status and never throws.  Status values are the reference
+ * library's ErrorCode numbers (ZKX/cusignal_cpp/include/cusignal/runtime/errors.h:18-41)
+ * so a C++ shim can rethrow them unchanged.  Complex data are interleaved
+ * complex64 (float re, float im), the layout of the reference's ComplexFloat and
+ * TypedComplex<float> (include/cusignal/backends/fft/fft_interface.h:104-107,
+ * include/cusignal/operators/filtering/filtering_typed.h:13).
+ *
+ * Pointers named x/y/out/threshold/... are device pointers.  Calls are
+ * asynchronous on `stream` (NULL = the legacy default stream, which is what the
+ * reference uses everywhere); host-side parameter errors are reported before any
+ * work is queued.  The last failure's message is available per host thread from
+ * zkx_last_error().
+ *
+ * Transform lengths (nfft) must be powers of two from 1 to 16384.
+ */
+#ifndef ZKX_RD_H
+#define ZKX_RD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define ZKX_API __attribute__((visibility("default")))
+#else
+#define ZKX_API
+#endif
+
+typedef struct CUstream_st* zkx_stream_t; /* identical to cudaStream_t */
+
+enum {
+    ZKX_SUCCESS = 0,
+    ZKX_INVALID_ARGUMENT = 1001,
+    ZKX_INVALID_SHAPE = 1002,
+    ZKX_UNSUPPORTED_OPERATION = 1004,
+    ZKX_CUDA_RUNTIME_ERROR = 2002,
+    ZKX_OUT_OF_MEMORY = 2003,
+    ZKX_BACKEND_ERROR = 2099,
+    ZKX_INTERNAL_ERROR = 9001
+};
+
+/* Window kinds, numbered as the reference's RadarWindowKind
+ * (include/cusignal/operators/radartools/radartools_typed.h:59-65). */
+enum {
+    ZKX_WINDOW_NONE = 0,
+    ZKX_WINDOW_HANN = 1,
+    ZKX_WINDOW_HAMMING = 2,
+    ZKX_WINDOW_EXPLICIT_FP32 = 3,
+    ZKX_WINDOW_EXPLICIT_FP64 = 4
+};
+
+/* CA-CFAR evaluation modes. */
+enum {
+    /* Separable training-ring sums in FP32 with every cell whose power lies within
+     * 1e-5 (relative) of its threshold re-decided in FP64: the detection mask equals
+     * an FP64 CFAR evaluated on the same input. */
+    ZKX_CFAR_ACCURATE = 0,
+    /* The reference's FP32 integral image, summed in the reference's order: thresholds
+     * and mask are bit-identical to ca_cfar_typed_cpu<float>. */
+    ZKX_CFAR_COMPAT = 1
+};
+
+ZKX_API const char* zkx_last_error(void);
+ZKX_API const char* zkx_version(void);
+
+/* pulse_compression: y[p, :] = IFFT(FFT(x[p, :nfft]) * conj(FFT(w*h/||w*h||, nfft))).
+ * Replaces cusignal::pulse_compression_device<float>
+ * (include/cusignal/operators/radartools/radartools_typed.h:257-262; computation
+ * src/operators/radartools/radartools_typed.cu:184-223).
+ * x [num_pulses, samples_per_pulse] complex64, replica [replica_length] complex64,
+ * explicit_window [replica_length] float (only for the explicit kinds, else NULL),
+ * y [num_pulses, nfft] complex64; nfft = -1 means samples_per_pulse.
+ * Uses a library-owned per-device scratch buffer for the replica spectrum. */
+ZKX_API int zkx_pulse_compression_c64(const void* x, int num_pulses, int samples_per_pulse,
+                              const void* replica, int replica_length, int nfft, int normalize,
+                              int window_kind, const float* explicit_window, void* y,
+                              zkx_stream_t stream);
+
+/* The replica spectrum alone: spectrum[k] = conj(FFT(w*h/||w*h||, nfft))[k] / nfft,
+ * the per-bin factor that zkx_pulse_compression_spectrum_c64 applies.  Lets callers
+ * keep a spectrum resident per waveform (no counterpart call in the reference, which
+ * recomputes it inside radartools_typed.cu:199-215). */
+ZKX_API int zkx_replica_spectrum_c64(const void* replica, int replica_length, int nfft, int normalize,
+                             int window_kind, const float* explicit_window, void* spectrum,
+                             zkx_stream_t stream);
+
+/* pulse_compression with a precomputed spectrum from zkx_replica_spectrum_c64. */
+ZKX_API int zkx_pulse_compression_spectrum_c64(const void* x, int num_pulses, int samples_per_pulse,
+                                       int nfft, const void* spectrum, void* y,
+                                       zkx_stream_t stream);
+
+/* pulse_doppler: out[k, n] = sum_p w[p] x[p, n] exp(-2 pi i k p / nfft), nfft = -1 means
+ * num_pulses; optional power[k, n] = |out[k, n]|^2 (NULL to skip; out may also be NULL
+ * when only the power is wanted).  Replaces cusignal::pulse_doppler_device<float>
+ * (radartools_typed.h:294-311; computation radartools_typed.cu:225-244).
+ * x [num_pulses, samples_per_pulse] complex64, out [nfft, samples_per_pulse] complex64. */
+ZKX_API int zkx_pulse_doppler_c64(const void* x, int num_pulses, int samples_per_pulse, int nfft,
+                          int window_kind, const float* explicit_window, void* out,
+                          float* power, zkx_stream_t stream);
+
+/* CFAR threshold multiplier alpha = N_ref * (pfa^(-1/N_ref) - 1), on the host in FP64.
+ * Replaces cusignal::cfar_alpha_typed_cpu / cfar_alpha_device (radartools_typed.h:207-222,
+ * radartools_typed.cpp:592-617). */
+ZKX_API int zkx_cfar_alpha(double pfa, int reference_count, double* alpha);
+
+/* Number of training cells of a 2-D CA-CFAR window (radartools_typed.cpp:203-212). */
+ZKX_API int zkx_cfar_reference_count(int rank, int guard_rows, int guard_columns, int reference_rows,
+                             int reference_columns);
+
+/* 1-D (rank 1, columns ignored) or 2-D CA-CFAR on row-major FP32 input.  threshold
+ * is 0 where the window does not fit; detections[i] = x[i] > threshold[i] (0/1 bytes).
+ * Replaces cusignal::ca_cfar_device<float> (radartools_typed.h:173-195; computation
+ * radartools_typed.cu:128-170, validation radartools_typed.cpp:161-220).
+ * mode is ZKX_CFAR_ACCURATE or ZKX_CFAR_COMPAT; rank-1 input always uses the compat
+ * algorithm (a single FP32 prefix sum, as the reference).  Compat mode uses a
+ * library-owned per-device scratch buffer of rows*columns floats. */
+ZKX_API int zkx_ca_cfar_f32(const float* x, int rank, int rows, int columns, int guard_rows,
+                    int guard_columns, int reference_rows, int reference_columns, double pfa,
+                    int mode, float* threshold, uint8_t* detections, zkx_stream_t stream);
+
+/* Causal FIR along the last axis of [lines, n]: y[l, i] = sum_k b[k] x[l, i-k]
+ * (+ zi[l, i] for i < nb-1 when zi is given; then zf[l, j] receives the final state).
+ * Replaces cusignal::firfilter_device<float> / firfilter_fp32_resident_device
+ * (include/cusignal/operators/filtering/filtering_typed.h:552-567;
+ * computation src/operators/filtering/filtering_typed.cu:118-184). */
+ZKX_API int zkx_fir_f32(const float* b, int nb, const float* x, int lines, int n, const float* zi,
+                float* y, float* zf, zkx_stream_t stream);
+
+/* Output length of upfirdn: floor(((n-1)*up + nh - 1) / down) + 1
+ * (src/operators/filtering/filtering_typed.cpp:1091-1098). */
+ZKX_API long long zkx_upfirdn_length(int n, int nh, int up, int down);
+
+/* Causal polyphase upfirdn along the last axis of [lines, n] with zero extension.
+ * Replaces cusignal::upfirdn_device<float> (filtering_typed.h:745-749; computation
+ * filtering_typed.cu:597-645).  y is [lines, zkx_upfirdn_length(n, nh, up, down)]. */
+ZKX_API int zkx_upfirdn_f32(const float* h, int nh, const float* x, int lines, int n, int up,
+                    int down, float* y, zkx_stream_t stream);
+
+/* resample_poly layout after gcd reduction (filtering_typed.cpp:933-1044). */
+typedef struct {
+    int up, down;            /* reduced factors */
+    int identity;            /* 1 when up == down after reduction (a copy) */
+    int output_samples;      /* ceil(n * up / down) */
+    int coefficient_count;   /* taps of the designed (or given) filter */
+    int half_length;
+    int prefix_zeros;
+    int output_start;
+} zkx_resample_layout;
+
+ZKX_API int zkx_resample_poly_layout(int n, int up, int down, int custom_coefficients,
+                             int coefficient_count, zkx_resample_layout* layout);
+
+/* Default design: Kaiser(beta) windowed sinc, cutoff 1/max(up, down), scaled to
+ * sum to up, computed on the host in FP64 (filtering_typed.cpp:159-222).
+ * taps (host) must hold layout->coefficient_count doubles. */
+ZKX_API int zkx_resample_poly_design(const zkx_resample_layout* layout, double kaiser_beta,
+                             double* taps);
+
+/* Centred polyphase resampling along the last axis of [lines, n] with FP32 device
+ * taps (already scaled by up).  Replaces the compute half of
+ * cusignal::resample_poly_device<float> (filtering_typed.h:765-770;
+ * filtering_typed.cpp:2717-2779, filtering_typed.cu:661-681).  y is
+ * [lines, layout->output_samples]. */
+ZKX_API int zkx_resample_poly_f32(const float* x, int lines, int n, const zkx_resample_layout* layout,
+                          const float* taps, float* y, zkx_stream_t stream);
+
+/* ------------------------------------------------------------ the fused chain */
+
+/* Chain description: pulse_compression -> pulse_doppler (+|.|^2) -> 2-D CA-CFAR on one
+ * CPI, the path of the reference's Task1 steps 2-4 (ZKX/Task1/pipeline/src/steps/
+ * step2/step2.cu:7-47, step3/step3.cu:7-49, step4/step4.cu:22-100). */
+typedef struct {
+    int num_pulses;          /* P */
+    int samples_per_pulse;   /* N (range samples) */
+    int range_nfft;          /* -1: N */
+    int doppler_nfft;        /* -1: P */
+    int replica_length;
+    int normalize;
+    int range_window;        /* ZKX_WINDOW_* applied to the replica */
+    int doppler_window;      /* ZKX_WINDOW_* applied across pulses */
+    int guard_cells[2];      /* Doppler, range */
+    int reference_cells[2];  /* Doppler, range */
+    double pfa;
+    int cfar_mode;           /* ZKX_CFAR_ACCURATE or ZKX_CFAR_COMPAT */
+} zkx_rd_desc;
+
+typedef struct zkx_rd_plan_s* zkx_rd_plan;
+
+/* Creates a plan on the current device: validates the description, computes the
+ * replica spectrum and the Doppler window once and keeps them resident.
+ * replica: device [replica_length] complex64; explicit windows are device arrays
+ * (NULL unless the matching kind is explicit). */
+ZKX_API int zkx_rd_plan_create(const zkx_rd_desc* desc, const void* replica,
+                       const float* range_window, const float* doppler_window,
+                       zkx_stream_t stream, zkx_rd_plan* plan);
+ZKX_API int zkx_rd_plan_destroy(zkx_rd_plan plan);
+
+/* Output sizes of a plan: compressed [P, range_nfft], rd and power/threshold/detections
+ * [doppler_nfft, range_nfft]. */
+ZKX_API int zkx_rd_plan_shape(zkx_rd_plan plan, int* range_bins, int* doppler_bins);
+
+/* Runs the chain on one CPI x [P, N] complex64.  compressed may be NULL only if the
+ * caller does not need it (it is still produced internally in a plan-owned buffer);
+ * rd may be NULL to skip storing the complex range-Doppler map. */
+ZKX_API int zkx_rd_execute(zkx_rd_plan plan, const void* x, void* compressed, void* rd, float* power,
+                   float* threshold, uint8_t* detections, zkx_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZKX_RD_H */

@@ -1,0 +1,114 @@
+"""Host-side checks of the C ABI (no GPU needed): every declared symbol is exported,
+argument validation reports the reference's error codes before any device work, and the
+host-computed pieces (alpha, layouts, the default resample_poly design) equal the oracle."""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def L():
+    from zkx_dev_b200 import _lib
+    try:
+        _lib.lib()
+    except ImportError as e:
+        pytest.skip(str(e))
+    return _lib
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "zkx_rd.h")).read()
+    return sorted(set(re.findall(r"ZKX_API\s+[\w\s\*]+?\b(zkx_\w+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported(L):
+    syms = header_symbols()
+    assert len(syms) >= 19
+    lib = ctypes.CDLL(L.LIB_PATH)
+    for s in syms:
+        assert hasattr(lib, s), f"{s} declared in include/zkx_rd.h but not exported"
+    assert set(syms) <= set(L.SIGNATURES), "ctypes signatures missing for some symbols"
+
+
+def test_pulse_compression_validation_codes(L):
+    lib = L.lib()
+    p = ctypes.c_void_p(16)  # never dereferenced: validation fails first
+    assert lib.zkx_pulse_compression_c64(p, 0, 16, p, 4, -1, 1, 0, None, p, None) == L.INVALID_SHAPE
+    assert lib.zkx_pulse_compression_c64(p, 2, 16, p, 0, -1, 1, 0, None, p, None) == L.INVALID_SHAPE
+    assert lib.zkx_pulse_compression_c64(p, 2, 16, p, 4, -1, 1, 7, None, p, None) == L.INVALID_ARGUMENT
+    assert lib.zkx_pulse_compression_c64(p, 2, 16, p, 4, -1, 1, 3, None, p, None) == L.INVALID_ARGUMENT
+    assert lib.zkx_pulse_compression_c64(p, 2, 16, p, 4, -1, 1, 0, p, p, None) == L.INVALID_ARGUMENT
+    assert lib.zkx_pulse_compression_c64(p, 2, 24, p, 4, -1, 1, 0, None, p, None) == L.UNSUPPORTED_OPERATION
+    assert lib.zkx_pulse_compression_c64(None, 2, 16, p, 4, -1, 1, 0, None, p, None) == L.INVALID_ARGUMENT
+    assert lib.zkx_pulse_compression_c64(p, 1 << 16, 1 << 16, p, 4, -1, 1, 0, None, p, None) == L.INVALID_SHAPE
+    assert b"pulse_compression" in lib.zkx_last_error()
+
+
+def test_doppler_and_cfar_validation_codes(L):
+    lib = L.lib()
+    p = ctypes.c_void_p(16)
+    assert lib.zkx_pulse_doppler_c64(p, 0, 8, -1, 0, None, p, None, None) == L.INVALID_SHAPE
+    assert lib.zkx_pulse_doppler_c64(p, 8, 8, 12, 0, None, p, None, None) == L.UNSUPPORTED_OPERATION
+    assert lib.zkx_pulse_doppler_c64(p, 8, 8, -1, 2, p, p, None, None) == L.INVALID_ARGUMENT
+    # window too large for the input: rows <= 2 * (guard + train)
+    assert lib.zkx_ca_cfar_f32(p, 2, 20, 100, 2, 2, 8, 8, 1e-3, 0, p, p, None) == L.INVALID_SHAPE
+    assert lib.zkx_ca_cfar_f32(p, 2, 100, 100, 2, 2, 0, 8, 1e-3, 0, p, p, None) == L.INVALID_ARGUMENT
+    assert lib.zkx_ca_cfar_f32(p, 2, 100, 100, 2, 2, 8, 8, 0.0, 0, p, p, None) == L.INVALID_ARGUMENT
+    assert lib.zkx_ca_cfar_f32(p, 2, 100, 100, 2, 2, 8, 8, 1.5, 0, p, p, None) == L.INVALID_ARGUMENT
+    assert lib.zkx_ca_cfar_f32(p, 3, 100, 100, 2, 2, 8, 8, 1e-3, 0, p, p, None) == L.INVALID_SHAPE
+    assert lib.zkx_ca_cfar_f32(p, 2, 100, 100, 2, 2, 8, 8, 1e-3, 9, p, p, None) == L.INVALID_ARGUMENT
+
+
+def test_filter_validation_codes(L):
+    lib = L.lib()
+    p = ctypes.c_void_p(16)
+    assert lib.zkx_fir_f32(p, 0, p, 1, 10, None, p, None, None) == L.INVALID_ARGUMENT
+    assert lib.zkx_fir_f32(p, 3, p, 0, 10, None, p, None, None) == L.INVALID_SHAPE
+    assert lib.zkx_upfirdn_f32(p, 0, p, 1, 10, 1, 1, p, None) == L.INVALID_ARGUMENT
+    assert lib.zkx_upfirdn_f32(p, 3, p, 1, 10, 0, 1, p, None) == L.INVALID_ARGUMENT
+    lay = L.ResampleLayout()
+    assert lib.zkx_resample_poly_layout(10, 0, 1, 0, 0, ctypes.byref(lay)) == L.INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("pfa,n", [(1e-6, 416), (1e-3, 128), (0.5, 1), (1.0, 16384), (1e-9, 2)])
+def test_cfar_alpha_matches_oracle(L, pfa, n):
+    a = ctypes.c_double()
+    assert L.lib().zkx_cfar_alpha(pfa, n, ctypes.byref(a)) == 0
+    assert a.value == O.cfar_alpha(pfa, n)
+
+
+@pytest.mark.parametrize("n,nh,up,down", [(100, 5, 2, 1), (1024, 7, 3, 2), (100, 9, 2, 3), (1, 1, 1, 1),
+                                          (0, 4, 3, 2), (1 << 20, 127, 3, 2)])
+def test_upfirdn_length_matches_oracle(L, n, nh, up, down):
+    assert L.lib().zkx_upfirdn_length(n, nh, up, down) == O.upfirdn_length(n, nh, up, down)
+
+
+@pytest.mark.parametrize("n,up,down", [(100, 3, 2), (10, 2, 1), (100, 2, 3), (1000, 1, 4), (77, 5, 3),
+                                       (32, 2, 2), (1 << 20, 3, 2), (50, 6, 4)])
+def test_resample_layout_and_design_match_oracle(L, n, up, down):
+    lay = L.ResampleLayout()
+    assert L.lib().zkx_resample_poly_layout(n, up, down, 0, 0, ctypes.byref(lay)) == 0
+    ref = O.resample_poly_layout(n, up, down)
+    for f, _ in L.ResampleLayout._fields_:
+        assert getattr(lay, f) == getattr(ref, f), f
+    if not lay.identity:
+        taps = np.zeros(lay.coefficient_count)
+        assert L.lib().zkx_resample_poly_design(ctypes.byref(lay), 5.0, taps.ctypes.data) == 0
+        np.testing.assert_array_equal(taps, O.resample_poly_design(n, up, down, 5.0))
+
+
+def test_reference_design_matches_restatement(reference_lib):
+    """The reference's own resample_poly on a small case equals the restatement."""
+    x = np.random.default_rng(0).standard_normal((2, 300)).astype(np.float32)
+    got, is64 = O.ref_resample_poly(x, 3, 2)
+    assert is64
+    np.testing.assert_array_equal(got, O.resample_poly(x, 3, 2))

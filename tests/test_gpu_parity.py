@@ -1,0 +1,276 @@
+"""GPU parity: the CUDA kernels (through libzkx_rd.so) against the oracle.
+
+Tolerances: the reference's FP32 path defines parity as relative L2 <= 1e-5 (the
+north-star bar for the plain FP32 path); max relative error against the FP64 oracle is
+checked per output; detection masks are compared exactly.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+REL_L2 = 1e-5
+
+
+def rel_l2(a, b) -> float:
+    a = np.asarray(a, dtype=np.complex128 if np.iscomplexobj(a) or np.iscomplexobj(b) else np.float64)
+    b = np.asarray(b, dtype=a.dtype)
+    den = np.linalg.norm(b.ravel())
+    return float(np.linalg.norm((a - b).ravel()) / (den if den > 0 else 1.0))
+
+
+@pytest.fixture(scope="module")
+def z():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import zkx_dev_b200
+    return zkx_dev_b200
+
+
+def dev(a):
+    return torch.as_tensor(np.ascontiguousarray(a)).cuda()
+
+
+def cplx(rng, *shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+# ------------------------------------------------------------ pulse compression
+
+@pytest.mark.parametrize("P,N,L,nfft", [(4, 64, 16, -1), (3, 256, 64, 256), (8, 1024, 100, -1),
+                                        (2, 300, 17, 512), (5, 4096, 256, -1), (2, 1000, 64, 256),
+                                        (1, 16, 4, 16), (7, 32, 32, 32), (3, 2048, 128, -1),
+                                        (2, 8192, 512, -1), (1, 16384, 1024, -1)])
+@pytest.mark.parametrize("window", ["none", "hamming", "hann"])
+def test_pulse_compression_matches_reference(z, P, N, L, nfft, window):
+    rng = np.random.default_rng(P * 1000 + N + L)
+    x, t = cplx(rng, P, N), cplx(rng, L)
+    nf = N if nfft == -1 else nfft
+    if P * nf * min(L, nf) > 5e7:
+        ref = O.pulse_compression_fft64(x, t, nfft, True, O.radar_window_f32(window, L) if window != "none" else None)
+    else:
+        ref = O.pulse_compression_direct(x, t, nfft, True, window)
+    got = z.pulse_compression(dev(x), dev(t), normalize=True,
+                              window=None if window == "none" else window,
+                              nfft=None if nfft == -1 else nfft).cpu().numpy()
+    assert got.shape == ref.shape
+    assert rel_l2(got, ref) <= REL_L2
+
+
+def test_pulse_compression_explicit_window_and_unnormalized(z):
+    rng = np.random.default_rng(7)
+    x, t = cplx(rng, 6, 512), cplx(rng, 40)
+    w = rng.uniform(0.2, 1.0, 40).astype(np.float32)
+    ref = O.pulse_compression_direct(x, t, -1, False, "explicit_fp32", w)
+    got = z.pulse_compression(dev(x), dev(t), normalize=False, window=dev(w)).cpu().numpy()
+    assert rel_l2(got, ref) <= REL_L2
+
+
+def test_pulse_compression_published_probe_inputs(z):
+    """The reference probe's own deterministic inputs (radartools_operator_probe.cu:36)."""
+    from tests.test_oracle_published import complex_input
+    x = complex_input(64 * 256, 3).reshape(64, 256)
+    t = complex_input(64, 7)
+    ref = O.pulse_compression_direct(x, t, 256, False)
+    got = z.pulse_compression(dev(x), dev(t), normalize=False, nfft=256).cpu().numpy()
+    assert rel_l2(got, ref) <= REL_L2
+
+
+def test_pulse_compression_identity_replica_full_size(z):
+    """Size-independent property at the 1024 x 16384 scale: a unit replica leaves
+    every pulse unchanged (FFT followed by its inverse)."""
+    rng = np.random.default_rng(11)
+    x = dev(cplx(rng, 1024, 16384))
+    one = dev(np.array([1.0 + 0j], dtype=np.complex64))
+    y = z.pulse_compression(x, one, normalize=True)
+    err = (torch.linalg.vector_norm(y - x) / torch.linalg.vector_norm(x)).item()
+    assert err <= 1e-6
+
+
+def test_pulse_compression_sampled_rows_vs_fp64_full_size(z):
+    """1024 x 16384 with a 1024-sample Hamming-windowed chirp: 8 sampled pulses against
+    the FP64 FFT oracle."""
+    from zkx_dev_b200.synth import make_cpi
+    cpi = make_cpi(1024, 16384, 8, 1024, seed=5)
+    y = z.pulse_compression(dev(cpi.x), dev(cpi.replica), normalize=True, window="hamming")
+    rows = [0, 1, 100, 511, 512, 777, 1022, 1023]
+    w = O.radar_window_f32("hamming", 1024)
+    ref = O.pulse_compression_fft64(cpi.x[rows], cpi.replica, -1, True, w)
+    got = y[rows].cpu().numpy()
+    assert rel_l2(got, ref) <= REL_L2
+
+
+# ------------------------------------------------------------------ Doppler
+
+@pytest.mark.parametrize("P,N,nfft", [(16, 16, -1), (32, 100, -1), (128, 129, -1), (64, 40, 128),
+                                      (100, 33, 128), (8, 17, 8), (256, 48, -1), (1024, 20, -1),
+                                      (2048, 16, -1), (512, 64, 256)])
+@pytest.mark.parametrize("window", ["none", "hamming"])
+def test_pulse_doppler_matches_reference(z, P, N, nfft, window):
+    rng = np.random.default_rng(P + N)
+    x = cplx(rng, P, N)
+    ref = O.pulse_doppler_direct(x, nfft, window)
+    got, power = z.pulse_doppler(dev(x), window=None if window == "none" else window,
+                                 nfft=None if nfft == -1 else nfft, return_power=True)
+    got = got.cpu().numpy()
+    assert got.shape == ref.shape
+    assert rel_l2(got, ref) <= REL_L2
+    assert rel_l2(power.cpu().numpy(), np.abs(got.astype(np.complex128)) ** 2) <= 1e-6
+
+
+def test_pulse_doppler_full_size_sampled_columns(z):
+    rng = np.random.default_rng(3)
+    x = cplx(rng, 1024, 16384)
+    rd = z.pulse_doppler(dev(x), window="hamming").cpu().numpy()
+    cols = [0, 1, 15, 16, 4097, 16383]
+    w = O.radar_window_f32("hamming", 1024)
+    ref, _ = O.pulse_doppler_fft64(x[:, cols], -1, w)
+    assert rel_l2(rd[:, cols], ref) <= REL_L2
+
+
+# ------------------------------------------------------------------- CFAR
+
+@pytest.mark.parametrize("shape,guard,train", [((64, 96), (2, 2), (8, 8)), ((40, 50), (1, 1), (4, 4)),
+                                               ((128, 4096), (2, 2), (8, 8)), ((33, 70), (2, 2), (4, 4)),
+                                               ((30, 31), (1, 2), (3, 5)), ((16, 16), (1, 1), (4, 4))])
+def test_ca_cfar_accurate_mask_equals_fp64(z, shape, guard, train):
+    rng = np.random.default_rng(shape[0] * shape[1])
+    p = rng.exponential(size=shape).astype(np.float32)
+    p[rng.integers(0, shape[0], 5), rng.integers(0, shape[1], 5)] *= 50.0
+    thr, det = z.ca_cfar(dev(p), list(guard), list(train), pfa=1e-3)
+    t64, m64 = O.ca_cfar_f64(p, guard, train, 1e-3)
+    np.testing.assert_array_equal(det.cpu().numpy().astype(np.uint8), m64)
+    got = thr.cpu().numpy().astype(np.float64)
+    nz = t64 > 0
+    assert np.max(np.abs(got[nz] - t64[nz]) / t64[nz]) <= 1e-5
+    assert np.all(got[~nz] == 0)
+
+
+def test_ca_cfar_near_threshold_cells_follow_fp64(z):
+    """Cells planted at the FP64 threshold (+-1 ulp-ish) must be decided as FP64 does."""
+    rng = np.random.default_rng(99)
+    p = rng.exponential(size=(64, 128)).astype(np.float32)
+    t64, _ = O.ca_cfar_f64(p, (2, 2), (8, 8), 1e-3)
+    cells = [(20, 30), (31, 64), (40, 100), (25, 77)]
+    for k, (r, c) in enumerate(cells):
+        t = t64[r, c]
+        p[r, c] = np.nextafter(np.float32(t), np.float32(np.inf if k % 2 else 0))
+    t64, m64 = O.ca_cfar_f64(p, (2, 2), (8, 8), 1e-3)
+    _, det = z.ca_cfar(dev(p), [2, 2], [8, 8], pfa=1e-3)
+    np.testing.assert_array_equal(det.cpu().numpy().astype(np.uint8), m64)
+
+
+@pytest.mark.parametrize("shape,guard,train", [((40, 50), (1, 1), (4, 4)), ((128, 256), (2, 2), (8, 8)),
+                                               ((100,), (1,), (5,)), ((128, 128), (1, 1), (4, 4))])
+def test_ca_cfar_compat_bit_exact(z, shape, guard, train):
+    rng = np.random.default_rng(len(shape) * 7 + shape[0])
+    p = rng.exponential(size=shape).astype(np.float32)
+    thr, det = z.ca_cfar(dev(p), list(guard), list(train), pfa=1e-3, mode="compat")
+    t_ref, d_ref = O.ca_cfar_compat(p, guard, train, 1e-3)
+    np.testing.assert_array_equal(thr.cpu().numpy(), t_ref)
+    np.testing.assert_array_equal(det.cpu().numpy().astype(np.uint8), d_ref)
+
+
+def test_ca_cfar_all_ones_known_answer(z):
+    """cuSignal test_radartools.py known answer: on unit input the threshold is alpha in
+    the interior and 0 at the borders."""
+    for shape, guard, train in [((10, 10), (1, 1), (2, 2)), ((10, 100), (1, 10), (2, 20))]:
+        ones = np.ones(shape, dtype=np.float32)
+        nref = O.reference_count_2d(guard, train)
+        alpha = z.cfar_alpha(1e-3, nref)
+        thr, _ = z.ca_cfar(dev(ones), list(guard), list(train), pfa=1e-3)
+        thr = thr.cpu().numpy()
+        mr, mc = guard[0] + train[0], guard[1] + train[1]
+        np.testing.assert_allclose(thr[mr:-mr, mc:-mc], alpha, rtol=1e-6)
+        assert np.all(thr[:mr] == 0) and np.all(thr[:, :mc] == 0)
+
+
+# ------------------------------------------------------------------ filters
+
+@pytest.mark.parametrize("nb,rows,n", [(9, 1, 10000), (127, 4, 20000), (1, 2, 100), (33, 3, 5000),
+                                       (127, 1, 100), (200, 2, 4097)])
+def test_firfilter_matches_reference(z, nb, rows, n):
+    rng = np.random.default_rng(nb + n)
+    b = rng.standard_normal(nb).astype(np.float32)
+    x = rng.standard_normal((rows, n)).astype(np.float32)
+    ref = O.firfilter(b, x)
+    got = z.firfilter(dev(b), dev(x)).cpu().numpy()
+    assert rel_l2(got, ref) <= REL_L2
+
+
+def test_firfilter_with_state(z):
+    rng = np.random.default_rng(5)
+    b = rng.standard_normal(17).astype(np.float32)
+    x = rng.standard_normal((3, 300)).astype(np.float32)
+    zi = rng.standard_normal((3, 16)).astype(np.float32)
+    y_ref, zf_ref = O.firfilter(b, x, zi)
+    y, zf = z.firfilter(dev(b), dev(x), zi=dev(zi))
+    assert rel_l2(y.cpu().numpy(), y_ref) <= REL_L2
+    assert rel_l2(zf.cpu().numpy(), zf_ref) <= REL_L2
+
+
+@pytest.mark.parametrize("nh,up,down,rows,n", [(127, 3, 2, 2, 5000), (5, 2, 1, 1, 100), (7, 3, 2, 32, 32),
+                                               (9, 2, 3, 100, 100), (61, 1, 4, 2, 999), (8, 5, 3, 1, 1)])
+def test_upfirdn_matches_reference(z, nh, up, down, rows, n):
+    rng = np.random.default_rng(nh * up + down)
+    h = rng.standard_normal(nh).astype(np.float32)
+    x = rng.standard_normal((rows, n)).astype(np.float32)
+    ref = O.upfirdn(h, x, up, down)
+    got = z.upfirdn(dev(h), dev(x), up, down).cpu().numpy()
+    assert got.shape == ref.shape
+    assert rel_l2(got, ref) <= REL_L2
+
+
+@pytest.mark.parametrize("up,down,rows,n", [(3, 2, 2, 5000), (2, 1, 10, 10), (2, 3, 100, 100),
+                                            (1, 4, 3, 1000), (5, 3, 1, 77)])
+def test_resample_poly_default_design_matches_reference(z, up, down, rows, n):
+    rng = np.random.default_rng(up * 10 + down)
+    x = rng.standard_normal((rows, n)).astype(np.float32)
+    ref = O.resample_poly(x, up, down)
+    got = z.resample_poly(dev(x), up, down, axis=-1).cpu().numpy()
+    assert got.shape == ref.shape
+    assert rel_l2(got, ref) <= REL_L2
+
+
+def test_resample_poly_custom_and_axis0(z):
+    rng = np.random.default_rng(17)
+    x = rng.standard_normal((100, 100)).astype(np.float32)
+    h = np.array([1, 2, 3, 2, 1], dtype=np.float32)
+    ref = O.resample_poly_custom_f32(x.T.copy(), 2, 3, h * np.float32(2)).T
+    got = z.resample_poly(dev(x), 2, 3, axis=0, window=h).cpu().numpy()
+    assert rel_l2(got, ref) <= REL_L2
+
+
+# ------------------------------------------------------------------- chain
+
+def test_chain_config1_against_fp64(z):
+    """128 x 4096 CPI, 20 targets, L = 256 Hamming replica, Hamming Doppler, CFAR 2/2 8/8
+    pfa 1e-6: every stage against the FP64 oracle and the mask against an FP64 CFAR of
+    the GPU's own power."""
+    from zkx_dev_b200.synth import make_cpi, seed_for
+    cpi = make_cpi(128, 4096, 20, 256, seed_for(1))
+    cfg = z.ChainConfig(128, 4096, 256)
+    chain = z.RangeDopplerChain(cfg, dev(cpi.replica))
+    out = chain(dev(cpi.x))
+    torch.cuda.synchronize()
+    w_r = O.radar_window_f32("hamming", 256)
+    w_d = O.radar_window_f32("hamming", 128)
+    comp64 = O.pulse_compression_fft64(cpi.x, cpi.replica, -1, True, w_r)
+    rd64, pow64 = O.pulse_doppler_fft64(comp64, -1, w_d)
+    comp = out["compressed"].cpu().numpy()
+    rd = out["rd"].cpu().numpy()
+    power = out["power"].cpu().numpy()
+    assert rel_l2(comp, comp64) <= REL_L2
+    assert rel_l2(rd, rd64) <= REL_L2
+    assert rel_l2(power, pow64) <= REL_L2
+    t64, m64 = O.ca_cfar_f64(power, (2, 2), (8, 8), 1e-6)
+    np.testing.assert_array_equal(out["detections"].cpu().numpy(), m64)
+    # the planted targets are detected at their (Doppler, range) cells
+    det = out["detections"].cpu().numpy()
+    hits = sum(det[t.doppler_bin, t.delay] for t in cpi.targets if t.snr_db > 15)
+    assert hits >= 0.8 * sum(1 for t in cpi.targets if t.snr_db > 15)

@@ -1,0 +1,110 @@
+"""ctypes binding of libzkx_rd.so (include/zkx_rd.h).
+
+The library is the only compute path: if it is missing, importing an operator raises
+immediately instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libzkx_rd.so")
+
+SUCCESS = 0
+INVALID_ARGUMENT = 1001
+INVALID_SHAPE = 1002
+UNSUPPORTED_OPERATION = 1004
+
+WINDOW_NONE, WINDOW_HANN, WINDOW_HAMMING, WINDOW_EXPLICIT_FP32, WINDOW_EXPLICIT_FP64 = range(5)
+CFAR_ACCURATE, CFAR_COMPAT = 0, 1
+
+# Every symbol the header declares, with its ctypes signature.
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+
+
+class ResampleLayout(ctypes.Structure):
+    _fields_ = [("up", _I), ("down", _I), ("identity", _I), ("output_samples", _I),
+                ("coefficient_count", _I), ("half_length", _I), ("prefix_zeros", _I),
+                ("output_start", _I)]
+
+
+class RdDesc(ctypes.Structure):
+    _fields_ = [("num_pulses", _I), ("samples_per_pulse", _I), ("range_nfft", _I),
+                ("doppler_nfft", _I), ("replica_length", _I), ("normalize", _I),
+                ("range_window", _I), ("doppler_window", _I), ("guard_cells", _I * 2),
+                ("reference_cells", _I * 2), ("pfa", _D), ("cfar_mode", _I)]
+
+
+SIGNATURES = {
+    "zkx_last_error": (ctypes.c_char_p, []),
+    "zkx_version": (ctypes.c_char_p, []),
+    "zkx_pulse_compression_c64": (_I, [_P, _I, _I, _P, _I, _I, _I, _I, _P, _P, _P]),
+    "zkx_replica_spectrum_c64": (_I, [_P, _I, _I, _I, _I, _P, _P, _P]),
+    "zkx_pulse_compression_spectrum_c64": (_I, [_P, _I, _I, _I, _P, _P, _P]),
+    "zkx_pulse_doppler_c64": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, _P]),
+    "zkx_cfar_alpha": (_I, [_D, _I, ctypes.POINTER(_D)]),
+    "zkx_cfar_reference_count": (_I, [_I, _I, _I, _I, _I]),
+    "zkx_ca_cfar_f32": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _D, _I, _P, _P, _P]),
+    "zkx_fir_f32": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P]),
+    "zkx_upfirdn_length": (ctypes.c_longlong, [_I, _I, _I, _I]),
+    "zkx_upfirdn_f32": (_I, [_P, _I, _P, _I, _I, _I, _I, _P, _P]),
+    "zkx_resample_poly_layout": (_I, [_I, _I, _I, _I, _I, ctypes.POINTER(ResampleLayout)]),
+    "zkx_resample_poly_design": (_I, [ctypes.POINTER(ResampleLayout), _D, _P]),
+    "zkx_resample_poly_f32": (_I, [_P, _I, _I, ctypes.POINTER(ResampleLayout), _P, _P, _P]),
+    "zkx_rd_plan_create": (_I, [ctypes.POINTER(RdDesc), _P, _P, _P, _P, ctypes.POINTER(_P)]),
+    "zkx_rd_plan_destroy": (_I, [_P]),
+    "zkx_rd_plan_shape": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "zkx_rd_execute": (_I, [_P, _P, _P, _P, _P, _P, _P, _P]),
+}
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+class ZkxError(RuntimeError):
+    """A failing libzkx_rd call; `code` is the reference's ErrorCode number."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+class ZkxValueError(ZkxError, ValueError):
+    """Invalid shape or argument (the reference throws std::invalid_argument)."""
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m zkx_dev_b200.build`")
+        handle = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != SUCCESS:
+        msg = lib().zkx_last_error().decode(errors="replace")
+        if rc in (INVALID_ARGUMENT, INVALID_SHAPE):
+            raise ZkxValueError(rc, msg)
+        raise ZkxError(rc, msg)
+
+
+def stream_handle(stream=None) -> Optional[int]:
+    """Raw cudaStream_t of a torch stream (default: torch's current stream)."""
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def ptr(t) -> Optional[int]:
+    return None if t is None else t.data_ptr()

@@ -1,0 +1,104 @@
+"""The range-Doppler chain as one plan: pulse_compression -> pulse_doppler (+|.|^2)
+-> 2-D CA-CFAR, the path of the reference's Task1 steps 2-4
+(ZKX/Task1/pipeline/src/steps/step{2,3,4}/step*.cu).
+
+A plan keeps the replica spectrum and the Doppler window resident on the device;
+executing it launches three kernels on the current stream.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Dict, Optional, Sequence
+
+import torch
+
+from . import _lib as L
+from .radartools import _window, _complex_input
+
+
+@dataclass
+class ChainConfig:
+    num_pulses: int
+    samples_per_pulse: int
+    replica_length: int
+    range_nfft: int = -1
+    doppler_nfft: int = -1
+    normalize: bool = True
+    range_window: object = "hamming"
+    doppler_window: object = "hamming"
+    guard_cells: Sequence[int] = (2, 2)
+    reference_cells: Sequence[int] = (8, 8)
+    pfa: float = 1e-6
+    cfar_mode: str = "accurate"
+
+
+class RangeDopplerChain:
+    """Owns a zkx_rd_plan for one CPI shape and waveform."""
+
+    def __init__(self, cfg: ChainConfig, replica: torch.Tensor):
+        replica = _complex_input(replica, 1, "replica")
+        if replica.numel() != cfg.replica_length:
+            raise ValueError("replica length mismatch")
+        self.cfg = cfg
+        dev = replica.device
+        rk, rw = _window(cfg.range_window, cfg.replica_length, dev)
+        dk, dw = _window(cfg.doppler_window, cfg.num_pulses, dev)
+        d = L.RdDesc()
+        d.num_pulses = cfg.num_pulses
+        d.samples_per_pulse = cfg.samples_per_pulse
+        d.range_nfft = cfg.range_nfft
+        d.doppler_nfft = cfg.doppler_nfft
+        d.replica_length = cfg.replica_length
+        d.normalize = int(cfg.normalize)
+        d.range_window = rk
+        d.doppler_window = dk
+        d.guard_cells[0], d.guard_cells[1] = cfg.guard_cells
+        d.reference_cells[0], d.reference_cells[1] = cfg.reference_cells
+        d.pfa = cfg.pfa
+        d.cfar_mode = {"accurate": L.CFAR_ACCURATE, "compat": L.CFAR_COMPAT}[cfg.cfar_mode]
+        self._keep = (replica, rw, dw)
+        h = ctypes.c_void_p()
+        L.check(L.lib().zkx_rd_plan_create(ctypes.byref(d), replica.data_ptr(), L.ptr(rw),
+                                           L.ptr(dw), L.stream_handle(), ctypes.byref(h)))
+        self._plan = h
+        nr, nd = ctypes.c_int(), ctypes.c_int()
+        L.check(L.lib().zkx_rd_plan_shape(h, ctypes.byref(nr), ctypes.byref(nd)))
+        self.range_bins, self.doppler_bins = nr.value, nd.value
+        self.device = dev
+
+    def allocate_outputs(self, keep_compressed: bool = True, keep_rd: bool = True) -> Dict[str, Optional[torch.Tensor]]:
+        P, nr, nd = self.cfg.num_pulses, self.range_bins, self.doppler_bins
+        dev = self.device
+        return {
+            "compressed": torch.empty((P, nr), dtype=torch.complex64, device=dev) if keep_compressed else None,
+            "rd": torch.empty((nd, nr), dtype=torch.complex64, device=dev) if keep_rd else None,
+            "power": torch.empty((nd, nr), dtype=torch.float32, device=dev),
+            "threshold": torch.empty((nd, nr), dtype=torch.float32, device=dev),
+            "detections": torch.empty((nd, nr), dtype=torch.uint8, device=dev),
+        }
+
+    def run(self, x: torch.Tensor, out: Optional[Dict[str, Optional[torch.Tensor]]] = None):
+        x = _complex_input(x, 2, "x")
+        if tuple(x.shape) != (self.cfg.num_pulses, self.cfg.samples_per_pulse):
+            raise ValueError("CPI shape does not match the plan")
+        if out is None:
+            out = self.allocate_outputs()
+        L.check(L.lib().zkx_rd_execute(self._plan, x.data_ptr(), L.ptr(out["compressed"]),
+                                       L.ptr(out["rd"]), L.ptr(out["power"]),
+                                       out["threshold"].data_ptr(), out["detections"].data_ptr(),
+                                       L.stream_handle()))
+        return out
+
+    __call__ = run
+
+    def close(self) -> None:
+        if getattr(self, "_plan", None) is not None and self._plan.value:
+            L.lib().zkx_rd_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,438 @@
+// extern "C" entry points of libzkx_rd.so: argument validation with the reference's
+// rules and error codes, then asynchronous kernel launches on the caller's stream.
+#include "fft_core.cuh"
+#include "zkx_internal.h"
+
+#include <climits>
+#include <cmath>
+#include <numeric>
+#include <string>
+
+using namespace zkx;
+
+namespace {
+
+constexpr int kMaxNfft = 1 << kMaxSmemFftLog;
+
+bool valid_window(int kind, const void* explicit_window)
+{
+    if (kind < ZKX_WINDOW_NONE || kind > ZKX_WINDOW_EXPLICIT_FP64) return false;
+    const bool is_explicit = kind == ZKX_WINDOW_EXPLICIT_FP32 || kind == ZKX_WINDOW_EXPLICIT_FP64;
+    return is_explicit == (explicit_window != nullptr);
+}
+
+int check_transform_length(int nfft, const char* fn)
+{
+    if (nfft < 1) return fail(ZKX_INVALID_ARGUMENT, std::string(fn) + ": nfft must be positive");
+    if (!is_pow2(nfft) || nfft > kMaxNfft)
+        return fail(ZKX_UNSUPPORTED_OPERATION,
+                    std::string(fn) + ": nfft must be a power of two no larger than 16384");
+    return ZKX_SUCCESS;
+}
+
+// radartools_typed.cpp:280-286: both extents >= 1 and the product fits an int.
+int check_radar_shape(int first, int second, const char* fn)
+{
+    const long long count = (long long)first * second;
+    if (first < 1 || second < 1 || count > INT_MAX)
+        return fail(ZKX_INVALID_SHAPE, std::string(fn) + " shape exceeds kernel capacity");
+    return ZKX_SUCCESS;
+}
+
+int compression_checks(const void* x, int P, int N, const void* replica, int L, int nfft,
+                       int kind, const float* w, const void* y)
+{
+    ZKX_TRY(check_radar_shape(P, N, "pulse_compression"));
+    ZKX_TRY(check_radar_shape(P, nfft, "pulse_compression"));
+    if (L < 1) return fail(ZKX_INVALID_SHAPE, "pulse_compression shape is invalid");
+    if (!valid_window(kind, w)) return fail(ZKX_INVALID_ARGUMENT, "pulse_compression window is invalid");
+    if (!x || !replica || !y) return fail(ZKX_INVALID_ARGUMENT, "pulse_compression: null pointer");
+    return check_transform_length(nfft, "pulse_compression");
+}
+
+struct CfarGeometry {
+    int nref = 0;
+    double alpha = 0.0;
+};
+
+// radartools_typed.cpp:161-220
+int cfar_checks(int rank, int rows, int cols, int gr, int gc, int rr, int rc, double pfa,
+                CfarGeometry* g)
+{
+    if (rank != 1 && rank != 2) return fail(ZKX_INVALID_SHAPE, "ca_cfar supports only 1D or 2D input here");
+    if (rows < 0 || (rank == 2 && cols < 0)) return fail(ZKX_INVALID_SHAPE, "ca_cfar shape dimensions must be nonnegative");
+    if (gr < 0 || rr < 1 || (rank == 2 && (gc < 0 || rc < 1)))
+        return fail(ZKX_INVALID_ARGUMENT, "ca_cfar guard/reference cells are invalid");
+    if ((long long)rows <= 2LL * ((long long)gr + rr) ||
+        (rank == 2 && (long long)cols <= 2LL * ((long long)gc + rc)))
+        return fail(ZKX_INVALID_SHAPE, "ca_cfar input dimension is too small");
+    if (!std::isfinite(pfa) || pfa <= 0.0 || pfa > 1.0) return fail(ZKX_INVALID_ARGUMENT, "ca_cfar pfa must be in (0,1]");
+    if ((long long)rows * (rank == 2 ? cols : 1) > INT_MAX)
+        return fail(ZKX_INVALID_SHAPE, "ca_cfar input size or capacity is invalid");
+    long long nref = rank == 2 ? 2LL * rr * (2LL * rc + 2LL * gc + 1) + 2LL * (2LL * gr + 1) * rc : 2LL * rr;
+    if (nref > INT_MAX) return fail(ZKX_INVALID_ARGUMENT, "ca_cfar reference count exceeds int capacity");
+    g->nref = (int)nref;
+    g->alpha = (double)nref * (std::pow(pfa, -1.0 / (double)nref) - 1.0);
+    return ZKX_SUCCESS;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ radar ops
+
+extern "C" int zkx_replica_spectrum_c64(const void* replica, int L, int nfft, int normalize,
+                                        int kind, const float* w, void* spectrum,
+                                        zkx_stream_t stream)
+{
+    if (L < 1) return fail(ZKX_INVALID_SHAPE, "replica length must be positive");
+    if (!valid_window(kind, w)) return fail(ZKX_INVALID_ARGUMENT, "replica window is invalid");
+    if (!replica || !spectrum) return fail(ZKX_INVALID_ARGUMENT, "replica_spectrum: null pointer");
+    ZKX_TRY(check_transform_length(nfft, "replica_spectrum"));
+    ZKX_TRY(ensure_device_ready());
+    return launch_replica_spectrum(static_cast<const float2*>(replica), L, nfft, normalize, kind, w,
+                                   static_cast<float2*>(spectrum), stream);
+}
+
+extern "C" int zkx_pulse_compression_spectrum_c64(const void* x, int P, int N, int nfft,
+                                                  const void* spectrum, void* y,
+                                                  zkx_stream_t stream)
+{
+    if (nfft == -1) nfft = N;
+    ZKX_TRY(check_radar_shape(P, N, "pulse_compression"));
+    ZKX_TRY(check_radar_shape(P, nfft, "pulse_compression"));
+    if (!x || !spectrum || !y) return fail(ZKX_INVALID_ARGUMENT, "pulse_compression: null pointer");
+    ZKX_TRY(check_transform_length(nfft, "pulse_compression"));
+    ZKX_TRY(ensure_device_ready());
+    return launch_pulse_compression(static_cast<const float2*>(x), P, N, nfft,
+                                    static_cast<const float2*>(spectrum), static_cast<float2*>(y),
+                                    stream);
+}
+
+extern "C" int zkx_pulse_compression_c64(const void* x, int P, int N, const void* replica, int L,
+                                         int nfft, int normalize, int kind, const float* w,
+                                         void* y, zkx_stream_t stream)
+{
+    if (nfft == -1) nfft = N;
+    ZKX_TRY(compression_checks(x, P, N, replica, L, nfft, kind, w, y));
+    ZKX_TRY(ensure_device_ready());
+    void* spec = nullptr;
+    ZKX_TRY(scratch(kScratchReplica, (size_t)nfft * sizeof(float2), &spec));
+    ZKX_TRY(launch_replica_spectrum(static_cast<const float2*>(replica), L, nfft, normalize, kind, w,
+                                    static_cast<float2*>(spec), stream));
+    return launch_pulse_compression(static_cast<const float2*>(x), P, N, nfft,
+                                    static_cast<const float2*>(spec), static_cast<float2*>(y), stream);
+}
+
+extern "C" int zkx_pulse_doppler_c64(const void* x, int P, int N, int nfft, int kind,
+                                     const float* w, void* out, float* power, zkx_stream_t stream)
+{
+    if (nfft == -1) nfft = P;
+    ZKX_TRY(check_radar_shape(P, N, "pulse_doppler"));
+    ZKX_TRY(check_radar_shape(nfft, N, "pulse_doppler"));
+    if (!valid_window(kind, w)) return fail(ZKX_INVALID_ARGUMENT, "pulse_doppler window is invalid");
+    if (!x || (!out && !power)) return fail(ZKX_INVALID_ARGUMENT, "pulse_doppler: null pointer");
+    ZKX_TRY(check_transform_length(nfft, "pulse_doppler"));
+    ZKX_TRY(ensure_device_ready());
+    float* win = nullptr;
+    if (kind != ZKX_WINDOW_NONE) {
+        void* p = nullptr;
+        ZKX_TRY(scratch(kScratchDopplerWindow, (size_t)P * sizeof(float), &p));
+        win = static_cast<float*>(p);
+        ZKX_TRY(launch_doppler_window(P, kind, w, win, stream));
+    }
+    return launch_pulse_doppler(static_cast<const float2*>(x), P, N, nfft, win,
+                                static_cast<float2*>(out), power, stream);
+}
+
+// ------------------------------------------------------------------------ CFAR
+
+extern "C" int zkx_cfar_alpha(double pfa, int reference_count, double* alpha)
+{
+    // radartools_typed.cpp:592-603
+    if (!alpha) return fail(ZKX_INVALID_ARGUMENT, "cfar_alpha: null pointer");
+    if (reference_count < 1 || !std::isfinite(pfa) || pfa <= 0.0 || pfa > 1.0)
+        return fail(ZKX_INVALID_ARGUMENT, "cfar_alpha requires reference >= 1 and pfa in (0,1]");
+    *alpha = (double)reference_count * (std::pow(pfa, -1.0 / (double)reference_count) - 1.0);
+    return ZKX_SUCCESS;
+}
+
+extern "C" int zkx_cfar_reference_count(int rank, int gr, int gc, int rr, int rc)
+{
+    if (rank == 1) return 2 * rr;
+    return 2 * rr * (2 * rc + 2 * gc + 1) + 2 * (2 * gr + 1) * rc;
+}
+
+extern "C" int zkx_ca_cfar_f32(const float* x, int rank, int rows, int cols, int gr, int gc,
+                               int rr, int rc, double pfa, int mode, float* threshold,
+                               uint8_t* detections, zkx_stream_t stream)
+{
+    CfarGeometry g;
+    ZKX_TRY(cfar_checks(rank, rows, cols, gr, gc, rr, rc, pfa, &g));
+    if (mode != ZKX_CFAR_ACCURATE && mode != ZKX_CFAR_COMPAT)
+        return fail(ZKX_INVALID_ARGUMENT, "ca_cfar: unknown mode");
+    if (!x || !threshold || !detections) return fail(ZKX_INVALID_ARGUMENT, "ca_cfar: null pointer");
+    ZKX_TRY(ensure_device_ready());
+    if (rank == 1 || mode == ZKX_CFAR_COMPAT) {
+        const long long count = (long long)rows * (rank == 2 ? cols : 1);
+        void* cum = nullptr;
+        ZKX_TRY(scratch(kScratchCfarIntegral, (size_t)count * sizeof(float), &cum));
+        return launch_ca_cfar_compat(x, rank, rows, rank == 2 ? cols : 1, gr, gc, rr, rc,
+                                     (float)g.alpha, g.nref, static_cast<float*>(cum), threshold,
+                                     detections, stream);
+    }
+    return launch_ca_cfar_accurate(x, rows, cols, gr, gc, rr, rc, g.alpha, g.nref, threshold,
+                                   detections, stream);
+}
+
+// --------------------------------------------------------------------- filters
+
+extern "C" int zkx_fir_f32(const float* b, int nb, const float* x, int lines, int n,
+                           const float* zi, float* y, float* zf, zkx_stream_t stream)
+{
+    // filtering_typed.cpp:1125-1146 (coefficients, shape) ...
+    if (nb < 1) return fail(ZKX_INVALID_ARGUMENT, "firfilter coefficients");
+    if (lines < 1 || n < 1 || (long long)lines * n > INT_MAX)
+        return fail(ZKX_INVALID_SHAPE, "firfilter input shape");
+    if (!b || !x || !y || (zi && nb > 1 && !zf)) return fail(ZKX_INVALID_ARGUMENT, "firfilter: null pointer");
+    ZKX_TRY(ensure_device_ready());
+    return launch_fir(b, nb, x, lines, n, zi, y, zi ? zf : nullptr, stream);
+}
+
+extern "C" long long zkx_upfirdn_length(int n, int nh, int up, int down)
+{
+    if (nh < 1 || up < 1 || down < 1 || n < 0) return -1;
+    const long long num = ((long long)n - 1) * up + nh - 1;
+    long long q = num / down;
+    if (num % down != 0 && num < 0) --q;
+    return q + 1;
+}
+
+extern "C" int zkx_upfirdn_f32(const float* h, int nh, const float* x, int lines, int n, int up,
+                               int down, float* y, zkx_stream_t stream)
+{
+    // filtering_typed.cpp:1046-1117
+    if (nh < 1) return fail(ZKX_INVALID_ARGUMENT, "upfirdn coefficients");
+    if (up < 1 || down < 1) return fail(ZKX_INVALID_ARGUMENT, "upfirdn factors");
+    if (lines < 1 || n < 0) return fail(ZKX_INVALID_SHAPE, "upfirdn input shape");
+    const long long nout = zkx_upfirdn_length(n, nh, up, down);
+    if (nout < 0 || nout > INT_MAX || (long long)lines * nout > INT_MAX)
+        return fail(ZKX_INVALID_SHAPE, "upfirdn output sample count");
+    if (!h || (!x && n > 0) || (!y && nout > 0)) return fail(ZKX_INVALID_ARGUMENT, "upfirdn: null pointer");
+    ZKX_TRY(ensure_device_ready());
+    return launch_polyphase(h, nh, up, down, 0, x, lines, n, y, (int)nout, stream);
+}
+
+extern "C" int zkx_resample_poly_layout(int n, int up, int down, int custom, int ncoeffs,
+                                        zkx_resample_layout* L)
+{
+    // filtering_typed.cpp:933-1044
+    if (!L) return fail(ZKX_INVALID_ARGUMENT, "resample_poly: null layout");
+    if (up < 1 || down < 1) return fail(ZKX_INVALID_ARGUMENT, "resample_poly factors");
+    if (n < 0) return fail(ZKX_INVALID_SHAPE, "resample_poly input shape");
+    *L = zkx_resample_layout{};
+    const int g = std::gcd(up, down);
+    L->up = up / g;
+    L->down = down / g;
+    L->identity = L->up == 1 && L->down == 1;
+    if (L->identity) {
+        L->output_samples = n;
+        return ZKX_SUCCESS;
+    }
+    const long long out = ((long long)n * L->up + L->down - 1) / L->down;
+    if (out > INT_MAX) return fail(ZKX_INVALID_SHAPE, "resample_poly output sample count");
+    L->output_samples = (int)out;
+    if (custom) {
+        if (ncoeffs < 0) return fail(ZKX_INVALID_ARGUMENT, "resample_poly coefficients");
+        L->coefficient_count = ncoeffs;
+        L->half_length = ncoeffs == 0 ? -1 : (ncoeffs - 1) / 2;
+    } else {
+        const int mr = L->up > L->down ? L->up : L->down;
+        if (mr > (INT_MAX - 1) / 20) return fail(ZKX_INVALID_ARGUMENT, "resample_poly designed filter length");
+        L->half_length = 10 * mr;
+        L->coefficient_count = 2 * L->half_length + 1;
+    }
+    const int rem = ((L->half_length % L->down) + L->down) % L->down;
+    L->prefix_zeros = L->down - rem;
+    L->output_start = (L->half_length + L->prefix_zeros) / L->down;
+    return ZKX_SUCCESS;
+}
+
+namespace {
+// Abramowitz-Stegun polynomial I0 used by the reference's design
+// (filtering_typed.cpp:159-174); kept so designed taps match the reference exactly.
+double bessel_i0_as(double v)
+{
+    const double a = std::fabs(v);
+    if (a < 3.75) {
+        const double r = v / 3.75, y = r * r;
+        return 1.0 + y * (3.5156229 + y * (3.0899424 + y * (1.2067492 + y * (0.2659732 +
+               y * (0.0360768 + y * 0.0045813)))));
+    }
+    const double y = 3.75 / a;
+    return std::exp(a) / std::sqrt(a) * (0.39894228 + y * (0.01328592 + y * (0.00225319 + y *
+           (-0.00157565 + y * (0.00916281 + y * (-0.02057706 + y * (0.02635537 + y *
+           (-0.01647633 + y * 0.00392377))))))));
+}
+}  // namespace
+
+extern "C" int zkx_resample_poly_design(const zkx_resample_layout* L, double beta, double* taps)
+{
+    // filtering_typed.cpp:176-222 (Kaiser window, windowed sinc, sum scaled to up)
+    if (!L || !taps) return fail(ZKX_INVALID_ARGUMENT, "resample_poly_design: null pointer");
+    const int count = L->coefficient_count, half = L->half_length;
+    if (count < 1 || half < 1) return fail(ZKX_INVALID_ARGUMENT, "resample_poly_design: empty design");
+    const double denom = bessel_i0_as(beta);
+    const double cutoff = 1.0 / (L->up > L->down ? L->up : L->down);
+    const double pi = 3.1415926535897932384626433832795;
+    double scale = 0.0;
+    for (int i = 0; i < count; ++i) {
+        const double ratio = (double)(i - half) / half;
+        const double bounded = std::max(0.0, 1.0 - ratio * ratio);
+        const double w = bessel_i0_as(beta * std::sqrt(bounded)) / denom;
+        const int off = i - half;
+        const double sinc = off == 0 ? cutoff : std::sin(pi * cutoff * off) / (pi * off);
+        taps[i] = sinc * w;
+        scale += taps[i];
+    }
+    for (int i = 0; i < count; ++i) taps[i] = taps[i] / scale * L->up;
+    return ZKX_SUCCESS;
+}
+
+extern "C" int zkx_resample_poly_f32(const float* x, int lines, int n, const zkx_resample_layout* L,
+                                     const float* taps, float* y, zkx_stream_t stream)
+{
+    if (!L) return fail(ZKX_INVALID_ARGUMENT, "resample_poly: null layout");
+    if (lines < 1 || n < 0 || (long long)lines * L->output_samples > INT_MAX)
+        return fail(ZKX_INVALID_SHAPE, "resample_poly workspace shape");
+    if (L->identity) {
+        if (n > 0) ZKX_CUDA(cudaMemcpyAsync(y, x, (size_t)lines * n * sizeof(float),
+                                            cudaMemcpyDeviceToDevice, stream));
+        return ZKX_SUCCESS;
+    }
+    if (L->coefficient_count < 1) return fail(ZKX_INVALID_ARGUMENT, "resample_poly coefficients");
+    if (!x || !taps || !y) return fail(ZKX_INVALID_ARGUMENT, "resample_poly: null pointer");
+    ZKX_TRY(ensure_device_ready());
+    const long long offset = (long long)L->output_start * L->down - L->prefix_zeros;
+    return launch_polyphase(taps, L->coefficient_count, L->up, L->down, offset, x, lines, n, y,
+                            L->output_samples, stream);
+}
+
+// ------------------------------------------------------------------ the chain
+
+struct zkx_rd_plan_s {
+    zkx_rd_desc d{};
+    int range_nfft = 0;
+    int doppler_nfft = 0;
+    int device = 0;
+    float2* spectrum = nullptr;
+    float* doppler_window = nullptr;
+    float2* compressed = nullptr;  // used when the caller passes no compressed buffer
+    float* power = nullptr;        // used when the caller passes no power buffer
+    float* cumulative = nullptr;   // compat CFAR integral image
+    CfarGeometry cfar;
+};
+
+namespace {
+void release_plan(zkx_rd_plan p)
+{
+    if (!p) return;
+    cudaFree(p->spectrum);
+    cudaFree(p->doppler_window);
+    cudaFree(p->compressed);
+    cudaFree(p->power);
+    cudaFree(p->cumulative);
+    delete p;
+}
+}  // namespace
+
+extern "C" int zkx_rd_plan_create(const zkx_rd_desc* d, const void* replica,
+                                  const float* range_window, const float* doppler_window,
+                                  zkx_stream_t stream, zkx_rd_plan* out)
+{
+    if (!d || !out || !replica) return fail(ZKX_INVALID_ARGUMENT, "rd_plan_create: null pointer");
+    *out = nullptr;
+    const int P = d->num_pulses, N = d->samples_per_pulse;
+    const int nr = d->range_nfft == -1 ? N : d->range_nfft;
+    const int nd = d->doppler_nfft == -1 ? P : d->doppler_nfft;
+    ZKX_TRY(compression_checks(replica, P, N, replica, d->replica_length, nr, d->range_window,
+                               range_window, replica));
+    ZKX_TRY(check_radar_shape(nd, nr, "pulse_doppler"));
+    if (!valid_window(d->doppler_window, doppler_window))
+        return fail(ZKX_INVALID_ARGUMENT, "pulse_doppler window is invalid");
+    ZKX_TRY(check_transform_length(nd, "pulse_doppler"));
+    if (d->cfar_mode != ZKX_CFAR_ACCURATE && d->cfar_mode != ZKX_CFAR_COMPAT)
+        return fail(ZKX_INVALID_ARGUMENT, "rd_plan: unknown CFAR mode");
+    CfarGeometry g;
+    ZKX_TRY(cfar_checks(2, nd, nr, d->guard_cells[0], d->guard_cells[1], d->reference_cells[0],
+                        d->reference_cells[1], d->pfa, &g));
+    ZKX_TRY(ensure_device_ready());
+    auto* p = new zkx_rd_plan_s;
+    p->d = *d;
+    p->range_nfft = nr;
+    p->doppler_nfft = nd;
+    p->cfar = g;
+    cudaGetDevice(&p->device);
+    cudaError_t e = cudaMalloc(&p->spectrum, (size_t)nr * sizeof(float2));
+    if (e == cudaSuccess && d->doppler_window != ZKX_WINDOW_NONE)
+        e = cudaMalloc(&p->doppler_window, (size_t)P * sizeof(float));
+    if (e == cudaSuccess && d->cfar_mode == ZKX_CFAR_COMPAT)
+        e = cudaMalloc(&p->cumulative, (size_t)nd * nr * sizeof(float));
+    if (e != cudaSuccess) {
+        release_plan(p);
+        return cuda_status(e, "rd_plan_create allocation");
+    }
+    int rc = launch_replica_spectrum(static_cast<const float2*>(replica), d->replica_length, nr,
+                                     d->normalize, d->range_window, range_window, p->spectrum, stream);
+    if (rc == ZKX_SUCCESS && p->doppler_window)
+        rc = launch_doppler_window(P, d->doppler_window, doppler_window, p->doppler_window, stream);
+    if (rc != ZKX_SUCCESS) {
+        release_plan(p);
+        return rc;
+    }
+    *out = p;
+    return ZKX_SUCCESS;
+}
+
+extern "C" int zkx_rd_plan_destroy(zkx_rd_plan plan)
+{
+    if (!plan) return ZKX_SUCCESS;
+    release_plan(plan);
+    return ZKX_SUCCESS;
+}
+
+extern "C" int zkx_rd_plan_shape(zkx_rd_plan plan, int* range_bins, int* doppler_bins)
+{
+    if (!plan) return fail(ZKX_INVALID_ARGUMENT, "rd_plan_shape: null plan");
+    if (range_bins) *range_bins = plan->range_nfft;
+    if (doppler_bins) *doppler_bins = plan->doppler_nfft;
+    return ZKX_SUCCESS;
+}
+
+extern "C" int zkx_rd_execute(zkx_rd_plan p, const void* x, void* compressed, void* rd,
+                              float* power, float* threshold, uint8_t* detections,
+                              zkx_stream_t stream)
+{
+    if (!p || !x || !threshold || !detections) return fail(ZKX_INVALID_ARGUMENT, "rd_execute: null pointer");
+    const int P = p->d.num_pulses, N = p->d.samples_per_pulse;
+    const int nr = p->range_nfft, nd = p->doppler_nfft;
+    if (!compressed) {
+        if (!p->compressed) ZKX_CUDA(cudaMalloc(&p->compressed, (size_t)P * nr * sizeof(float2)));
+        compressed = p->compressed;
+    }
+    if (!power) {
+        if (!p->power) ZKX_CUDA(cudaMalloc(&p->power, (size_t)nd * nr * sizeof(float)));
+        power = p->power;
+    }
+    ZKX_TRY(launch_pulse_compression(static_cast<const float2*>(x), P, N, nr, p->spectrum,
+                                     static_cast<float2*>(compressed), stream));
+    ZKX_TRY(launch_pulse_doppler(static_cast<const float2*>(compressed), P, nr, nd,
+                                 p->doppler_window, static_cast<float2*>(rd), power, stream));
+    const int* gd = p->d.guard_cells;
+    const int* rf = p->d.reference_cells;
+    if (p->d.cfar_mode == ZKX_CFAR_COMPAT)
+        return launch_ca_cfar_compat(power, 2, nd, nr, gd[0], gd[1], rf[0], rf[1],
+                                     (float)p->cfar.alpha, p->cfar.nref, p->cumulative, threshold,
+                                     detections, stream);
+    return launch_ca_cfar_accurate(power, nd, nr, gd[0], gd[1], rf[0], rf[1], p->cfar.alpha,
+                                   p->cfar.nref, threshold, detections, stream);
+}

@@ -1,0 +1,346 @@
+// 2-D cell-averaging CFAR for sm_100a, two modes.
+//
+// Accurate mode (the chain's default).  A CTA owns a 32 x 64 tile of cells and
+// stages the tile plus its (guard + training) halo in shared memory once.  The
+// training-ring sum of a cell is assembled from separable pieces that are all sums
+// of non-negative terms (no outer-minus-inner cancellation):
+//   A[r][c] = sum of the 2*RR training rows of column c around row r
+//   B[r][c] = sum of the 2*GR+1 guard rows of column c around row r
+//   ring    = sum_{|dc|<=MC} A[r][c+dc] + sum_{GC<|dc|<=MC} B[r][c+dc]
+// Every window sum is formed as (suffix of one W-block) + (prefix of the next), so a
+// window costs one add after two adds of preparation per element and its relative
+// error stays below W units in the last place.  The FP32 threshold is therefore
+// within ~3e-6 (relative) of the FP64 one; every cell whose power lies within 1e-5
+// of its threshold is re-decided with the ring summed in FP64, so the mask equals an
+// FP64 CFAR on the same input.
+//
+// Compat mode reproduces the reference's FP32 integral image bit for bit
+// (radartools_kernels.cuh:40-134): a column running sum, then a row running sum, in
+// the same order and with the same corner formula.  It exists for parity checks
+// against the reference; it is slower (the running sums are sequential).
+//
+// Algorithmic HBM traffic of the accurate kernel: 4 B read + 4 B threshold + 1 B
+// mask = 9 B per cell.
+#include "fft_core.cuh"
+#include "zkx_internal.h"
+
+namespace zkx {
+namespace {
+
+constexpr int kCfarTY = 32;
+constexpr int kCfarTX = 64;
+constexpr int kCfarThreads = 256;
+constexpr float kRecheckBand = 1e-5f;
+
+// out[i] = v[i] + ... + v[i+W-1], i in [0, LEN-W], as suffix(block) + prefix(next block).
+template <int W, int LEN>
+__device__ __forceinline__ void window_sums(const float* v, float* out)
+{
+    static_assert(LEN >= W && W >= 1, "window");
+    float pre[LEN], suf[LEN];
+    static_for<0, LEN>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        if constexpr (i % W == 0) pre[i] = v[i];
+        else pre[i] = pre[i - 1] + v[i];
+    });
+    static_for<0, LEN>([&](auto I) {
+        constexpr int i = LEN - 1 - decltype(I)::value;
+        constexpr int end = (i / W) * W + W - 1 < LEN - 1 ? (i / W) * W + W - 1 : LEN - 1;
+        if constexpr (i == end) suf[i] = v[i];
+        else suf[i] = suf[i + 1] + v[i];
+    });
+    static_for<0, LEN - W + 1>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        if constexpr (i % W == 0) out[i] = pre[i + W - 1];
+        else out[i] = suf[i] + pre[i + W - 1];
+    });
+}
+
+template <int GR, int GC, int RR, int RC>
+__global__ void __launch_bounds__(kCfarThreads)
+cfar_accurate_kernel(const float* __restrict__ x, int rows, int cols, float scale32,
+                     double scale64, float* __restrict__ thr, uint8_t* __restrict__ det)
+{
+    constexpr int MR = GR + RR, MC = GC + RC;
+    constexpr int TY = kCfarTY, TX = kCfarTX;
+    constexpr int HR = TY + 2 * MR, HC = TX + 2 * MC;
+    constexpr int SAP = HC | 1;  // odd row pitch: a warp walking 32 rows hits 32 banks
+    __shared__ float P[HR][SAP];
+    __shared__ float SA[TY][SAP];
+    __shared__ float SB[TY][SAP];
+    const int r0 = blockIdx.y * TY;
+    const int c0 = blockIdx.x * TX;
+
+    for (int i = threadIdx.x; i < HR * HC; i += kCfarThreads) {
+        const int hr = i / HC, hc = i - hr * HC;
+        const int gr = r0 - MR + hr, gc = c0 - MC + hc;
+        P[hr][hc] = (gr >= 0 && gr < rows && gc >= 0 && gc < cols) ? __ldg(&x[(size_t)gr * cols + gc]) : 0.f;
+    }
+    __syncthreads();
+
+    // vertical pieces: one thread per (halo column, 16-row segment)
+    constexpr int SEG = 16;
+    constexpr int VL = SEG + 2 * MR;
+    for (int item = threadIdx.x; item < HC * (TY / SEG); item += kCfarThreads) {
+        const int hc = item % HC;
+        const int rb = (item / HC) * SEG;
+        float v[VL];
+#pragma unroll
+        for (int i = 0; i < VL; ++i) v[i] = P[rb + i][hc];
+        float wt[VL - RR + 1], wg[VL - 2 * GR];
+        window_sums<RR, VL>(v, wt);
+        window_sums<2 * GR + 1, VL>(v, wg);
+#pragma unroll
+        for (int r = 0; r < SEG; ++r) {
+            SA[rb + r][hc] = wt[r] + wt[r + MR + GR + 1];
+            SB[rb + r][hc] = wg[r + MR - GR];
+        }
+    }
+    __syncthreads();
+
+    // horizontal: lane = row, warp = 8-column segment
+    constexpr int CS = TX / (kCfarThreads / TY);  // 8 columns per thread
+    constexpr int HL = CS + 2 * MC;
+    const int r = threadIdx.x % TY;
+    const int cb = (threadIdx.x / TY) * CS;
+    float a[HL], b[HL];
+#pragma unroll
+    for (int i = 0; i < HL; ++i) {
+        a[i] = SA[r][cb + i];
+        b[i] = SB[r][cb + i];
+    }
+    float wa[HL - 2 * MC], wb[HL - RC + 1];
+    window_sums<2 * MC + 1, HL>(a, wa);
+    window_sums<RC, HL>(b, wb);
+    const int grow = r0 + r;
+    if (grow >= rows) return;
+    const bool row_interior = grow >= MR && grow < rows - MR;
+    float tout[CS];
+    uint8_t dout[CS];
+#pragma unroll
+    for (int j = 0; j < CS; ++j) {
+        const int gcol = c0 + cb + j;
+        const float xv = P[r + MR][cb + j + MC];
+        float t = 0.f;
+        bool hit;
+        if (row_interior && gcol >= MC && gcol < cols - MC) {
+            const float ring = wa[j] + (wb[j] + wb[j + MC + GC + 1]);
+            t = scale32 * ring;
+            hit = xv > t;
+            if (fabsf(xv - t) <= kRecheckBand * t) {
+                double s = 0.0;
+                for (int dr = -MR; dr <= MR; ++dr)
+                    for (int dc = -MC; dc <= MC; ++dc)
+                        if (dr < -GR || dr > GR || dc < -GC || dc > GC)
+                            s += (double)P[r + MR + dr][cb + j + MC + dc];
+                const double t64 = scale64 * s;
+                hit = (double)xv > t64;
+                t = (float)t64;
+            }
+        } else {
+            hit = xv > 0.f;
+        }
+        tout[j] = t;
+        dout[j] = hit ? 1 : 0;
+    }
+    const int cstart = c0 + cb;
+    const bool thr_vec = ((reinterpret_cast<uintptr_t>(thr) & 15) == 0) && (cols & 3) == 0;
+    const bool det_vec = ((reinterpret_cast<uintptr_t>(det) & 7) == 0) && (cols & 7) == 0;
+    if (cstart + CS <= cols && thr_vec) {
+        float4* tp = reinterpret_cast<float4*>(thr + (size_t)grow * cols + cstart);
+        tp[0] = make_float4(tout[0], tout[1], tout[2], tout[3]);
+        tp[1] = make_float4(tout[4], tout[5], tout[6], tout[7]);
+        if (det_vec) {
+            uint2 packed;
+            packed.x = dout[0] | (dout[1] << 8) | (dout[2] << 16) | ((unsigned)dout[3] << 24);
+            packed.y = dout[4] | (dout[5] << 8) | (dout[6] << 16) | ((unsigned)dout[7] << 24);
+            *reinterpret_cast<uint2*>(det + (size_t)grow * cols + cstart) = packed;
+        } else {
+#pragma unroll
+            for (int j = 0; j < CS; ++j) det[(size_t)grow * cols + cstart + j] = dout[j];
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < CS; ++j) {
+            if (cstart + j < cols) {
+                thr[(size_t)grow * cols + cstart + j] = tout[j];
+                det[(size_t)grow * cols + cstart + j] = dout[j];
+            }
+        }
+    }
+}
+
+// Any window geometry: one thread per cell, ring summed directly in FP64.
+__global__ void cfar_generic_kernel(const float* __restrict__ x, int rows, int cols, int gr, int gc,
+                                    int rr, int rc, double scale64, float* __restrict__ thr,
+                                    uint8_t* __restrict__ det)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)rows * cols) return;
+    const int r = (int)(i / cols), c = (int)(i % cols);
+    const int mr = gr + rr, mc = gc + rc;
+    const float xv = x[i];
+    float t = 0.f;
+    bool hit;
+    if (r >= mr && r < rows - mr && c >= mc && c < cols - mc) {
+        double s = 0.0;
+        for (int dr = -mr; dr <= mr; ++dr)
+            for (int dc = -mc; dc <= mc; ++dc)
+                if (dr < -gr || dr > gr || dc < -gc || dc > gc) s += (double)x[(size_t)(r + dr) * cols + c + dc];
+        const double t64 = scale64 * s;
+        t = (float)t64;
+        hit = (double)xv > t64;
+    } else {
+        hit = xv > 0.f;
+    }
+    thr[i] = t;
+    det[i] = hit ? 1 : 0;
+}
+
+// --------------------------------------------------------------- compat mode
+
+__global__ void compat_column_cumsum_kernel(const float* __restrict__ x, int rows, int cols,
+                                            float* __restrict__ cum)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    float run = 0.f;
+    for (int r = 0; r < rows; ++r) {
+        run = __fadd_rn(run, x[(size_t)r * cols + c]);
+        cum[(size_t)r * cols + c] = run;
+    }
+}
+
+// One warp per 32 rows; 32 x 32 tiles are staged through shared memory so the
+// sequential row scan still reads and writes HBM in coalesced rows.
+__global__ void compat_row_cumsum_kernel(float* __restrict__ cum, int rows, int cols)
+{
+    __shared__ float tile[32][33];
+    const int lane = threadIdx.x;
+    const int r0 = blockIdx.x * 32;
+    float run = 0.f;
+    for (int c0 = 0; c0 < cols; c0 += 32) {
+        for (int i = 0; i < 32; ++i) {
+            const int rr = r0 + i, cc = c0 + lane;
+            tile[i][lane] = (rr < rows && cc < cols) ? cum[(size_t)rr * cols + cc] : 0.f;
+        }
+        __syncwarp();
+        for (int j = 0; j < 32 && c0 + j < cols; ++j) {
+            run = __fadd_rn(run, tile[lane][j]);
+            tile[lane][j] = run;
+        }
+        __syncwarp();
+        for (int i = 0; i < 32; ++i) {
+            const int rr = r0 + i, cc = c0 + lane;
+            if (rr < rows && cc < cols) cum[(size_t)rr * cols + cc] = tile[i][lane];
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void compat_cumsum_1d_kernel(const float* __restrict__ x, int n, float* __restrict__ cum)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    float run = 0.f;
+    for (int i = 0; i < n; ++i) {
+        run = __fadd_rn(run, x[i]);
+        cum[i] = run;
+    }
+}
+
+// Threshold from the integral image with the reference's operation order
+// (radartools_kernels.cuh:85-133); explicit _rn intrinsics keep nvcc from fusing.
+__global__ void compat_threshold_kernel(const float* __restrict__ x, const float* __restrict__ cum,
+                                        int rank, int rows, int cols, int gr, int gc, int rr,
+                                        int rc, float alpha, int nref, float* __restrict__ thr,
+                                        uint8_t* __restrict__ det)
+{
+    const long long index = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long count = (long long)rows * cols;
+    if (index >= count) return;
+    const float scale = __fdiv_rn(alpha, (float)nref);
+    float t = 0.f;
+    if (rank == 1) {
+        const int i = (int)index;
+        const int m = gr + rr;
+        if (i >= m && i < rows - m) {
+            const int orr = i + m, ol = i - m - 1, ir = i + gr, il = i - gr - 1;
+            const float outer = ol >= 0 ? __fsub_rn(cum[orr], cum[ol]) : cum[orr];
+            const float inner = __fsub_rn(cum[ir], cum[il]);
+            t = __fmul_rn(scale, __fsub_rn(outer, inner));
+        }
+    } else {
+        const int r = (int)(index / cols), c = (int)(index % cols);
+        const int rm = gr + rr, cm = gc + rc;
+        if (r >= rm && r < rows - rm && c >= cm && c < cols - cm) {
+#define AT(r_, c_) cum[(size_t)(r_) * cols + (c_)]
+            const int ot = r + rm, ol = r - rm - 1, orc = c + cm, olc = c - cm - 1;
+            float outer = AT(ot, orc);
+            if (ol >= 0) outer = __fsub_rn(outer, AT(ol, orc));
+            if (olc >= 0) outer = __fsub_rn(outer, AT(ot, olc));
+            if (ol >= 0 && olc >= 0) outer = __fadd_rn(outer, AT(ol, olc));
+            float inner = __fsub_rn(AT(r + gr, c + gc), AT(r - gr - 1, c + gc));
+            inner = __fsub_rn(inner, AT(r + gr, c - gc - 1));
+            inner = __fadd_rn(inner, AT(r - gr - 1, c - gc - 1));
+#undef AT
+            t = __fmul_rn(scale, __fsub_rn(outer, inner));
+        }
+    }
+    thr[index] = t;
+    det[index] = x[index] > t ? 1 : 0;
+}
+
+template <int GR, int GC, int RR, int RC>
+int accurate_impl(const float* x, int rows, int cols, float s32, double s64, float* thr,
+                  uint8_t* det, cudaStream_t s)
+{
+    dim3 grid((cols + kCfarTX - 1) / kCfarTX, (rows + kCfarTY - 1) / kCfarTY);
+    cfar_accurate_kernel<GR, GC, RR, RC><<<grid, kCfarThreads, 0, s>>>(x, rows, cols, s32, s64, thr, det);
+    ZKX_LAUNCHED("cfar_accurate_kernel");
+    return ZKX_SUCCESS;
+}
+
+}  // namespace
+
+int launch_ca_cfar_accurate(const float* x, int rows, int columns, int gr, int gc, int rr, int rc,
+                            double alpha, int nref, float* threshold, uint8_t* detections,
+                            cudaStream_t stream)
+{
+    const double s64 = alpha / (double)nref;
+    const float s32 = (float)s64;
+#define ZKX_CFAR_CASE(A, B, C, D) \
+    if (gr == A && gc == B && rr == C && rc == D) return accurate_impl<A, B, C, D>(x, rows, columns, s32, s64, threshold, detections, stream);
+    ZKX_CFAR_CASE(2, 2, 8, 8)
+    ZKX_CFAR_CASE(1, 1, 4, 4)
+    ZKX_CFAR_CASE(2, 2, 4, 4)
+    ZKX_CFAR_CASE(1, 1, 2, 2)
+#undef ZKX_CFAR_CASE
+    const long long count = (long long)rows * columns;
+    cfar_generic_kernel<<<(unsigned)((count + 255) / 256), 256, 0, stream>>>(
+        x, rows, columns, gr, gc, rr, rc, s64, threshold, detections);
+    ZKX_LAUNCHED("cfar_generic_kernel");
+    return ZKX_SUCCESS;
+}
+
+int launch_ca_cfar_compat(const float* x, int rank, int rows, int columns, int gr, int gc, int rr,
+                          int rc, float alpha, int nref, float* cum, float* threshold,
+                          uint8_t* detections, cudaStream_t stream)
+{
+    if (rank == 1) {
+        compat_cumsum_1d_kernel<<<1, 1, 0, stream>>>(x, rows, cum);
+        ZKX_LAUNCHED("compat_cumsum_1d_kernel");
+        columns = 1;
+    } else {
+        compat_column_cumsum_kernel<<<(columns + 255) / 256, 256, 0, stream>>>(x, rows, columns, cum);
+        ZKX_LAUNCHED("compat_column_cumsum_kernel");
+        compat_row_cumsum_kernel<<<(rows + 31) / 32, 32, 0, stream>>>(cum, rows, columns);
+        ZKX_LAUNCHED("compat_row_cumsum_kernel");
+    }
+    const long long count = (long long)rows * columns;
+    compat_threshold_kernel<<<(unsigned)((count + 255) / 256), 256, 0, stream>>>(
+        x, cum, rank, rows, columns, gr, gc, rr, rc, alpha, nref, threshold, detections);
+    ZKX_LAUNCHED("compat_threshold_kernel");
+    return ZKX_SUCCESS;
+}
+
+}  // namespace zkx

@@ -1,0 +1,291 @@
+// Range compression (fused FFT x conj(replica spectrum) x IFFT per pulse) and the
+// Doppler transform (windowed FFT across pulses, optional |.|^2) for sm_100a.
+//
+// Layout in HBM: a CPI is row-major [pulses, range samples] complex64; the
+// compressed cube keeps that layout ([pulses, range_nfft]); the range-Doppler map
+// and power are [doppler_nfft, range_nfft] (Doppler bin major), the reference's
+// output layout (radartools_typed.cu:241-243).
+//
+// Range compression reads each pulse once and writes it once: 16 B per cell of
+// compulsory HBM traffic.  The Doppler kernel reads the compressed cube once and
+// writes the map (8 B) and the power (4 B): 20 B per cell.
+#include "fft_core.cuh"
+#include "zkx_internal.h"
+
+namespace zkx {
+namespace {
+
+// Values per thread for a transform of length N (a plan table chosen so that every
+// pass but the last uses the full radix and the thread count stays in 8..512).
+constexpr int elems_for(int n)
+{
+    return n <= 32 ? n : n == 64 ? 8 : n == 128 ? 16 : n == 256 ? 16 : n == 512 ? 32
+         : n == 1024 ? 32 : n == 2048 ? 16 : n == 4096 ? 16 : 32;
+}
+
+// Transforms per CTA for row kernels: aim for >= 128 threads per CTA.
+constexpr int rows_per_cta(int n)
+{
+    constexpr int kTarget = 128;
+    const int t = n / elems_for(n);
+    return t >= kTarget ? 1 : kTarget / t;
+}
+
+__device__ __forceinline__ float window_value(int kind, const float* explicit_window, int i,
+                                              int length)
+{
+    // Hann/Hamming evaluated in FP64 and rounded once (the reference evaluates the
+    // same formulas in FP32, radartools_kernels.cuh:150-160).
+    if (kind == ZKX_WINDOW_EXPLICIT_FP32 || kind == ZKX_WINDOW_EXPLICIT_FP64) return explicit_window[i];
+    if (kind == ZKX_WINDOW_NONE || length <= 1) return 1.0f;
+    const double c = cospi(2.0 * (double)i / (double)(length - 1));
+    if (kind == ZKX_WINDOW_HANN) return (float)(0.5 - 0.5 * c);
+    return (float)(0.54 - 0.46 * c);
+}
+
+// ------------------------------------------------------------ replica spectrum
+
+// spectrum[k] = conj(FFT(w h / ||w h||, N))[k] / N; one CTA.  The norm runs over all
+// `length` template samples (radartools_typed.cpp:639-648) in FP64.
+template <int N>
+__global__ void __launch_bounds__(FftPlan<N, elems_for(N)>::T)
+replica_spectrum_kernel(const float2* __restrict__ h, int length, int normalize, int window_kind,
+                        const float* __restrict__ explicit_window, float2* __restrict__ spectrum,
+                        const float2* __restrict__ tw)
+{
+    using PL = FftPlan<N, elems_for(N)>;
+    extern __shared__ float2 sm[];
+    __shared__ double partial[PL::T];
+    const int t = threadIdx.x;
+    double acc = 0.0;
+    for (int i = t; i < length; i += PL::T) {
+        const double w = window_value(window_kind, explicit_window, i, length);
+        const float2 v = h[i];
+        const double re = (double)v.x * w, im = (double)v.y * w;
+        acc += re * re + im * im;
+    }
+    partial[t] = acc;
+    __syncthreads();
+    if (t == 0) {
+        double total = 0.0;
+        for (int i = 0; i < PL::T; ++i) total += partial[i];
+        partial[0] = total;
+    }
+    __syncthreads();
+    const double norm = normalize ? sqrt(partial[0]) : 1.0;
+    const float scale = (float)(1.0 / (norm * (double)N));
+    float2 v[PL::E];
+#pragma unroll
+    for (int r = 0; r < PL::E; ++r) {
+        const int e = t + PL::T * r;
+        float2 x = make_float2(0.f, 0.f);
+        if (e < length) {
+            const float w = window_value(window_kind, explicit_window, e, length);
+            const float2 hv = h[e];
+            x = make_float2(hv.x * w, hv.y * w);
+        }
+        v[r] = x;
+    }
+    fft_block<PL, -1, 1>(v, sm, t, tw);
+#pragma unroll
+    for (int r = 0; r < PL::E; ++r) {
+        const float2 s = v[r];
+        spectrum[t + PL::T * r] = make_float2(s.x * scale, -s.y * scale);
+    }
+}
+
+// ------------------------------------------------------------ range compression
+
+// G pulses per CTA; each pulse: load (zero-pad/truncate to N), forward FFT, multiply
+// by the replica spectrum, inverse FFT, store.  The cube crosses HBM once each way.
+template <int N, int G>
+__global__ void __launch_bounds__(G * FftPlan<N, elems_for(N)>::T)
+pulse_compression_kernel(const float2* __restrict__ x, int pulses, int samples,
+                         const float2* __restrict__ spectrum, float2* __restrict__ y,
+                         const float2* __restrict__ tw)
+{
+    using PL = FftPlan<N, elems_for(N)>;
+    extern __shared__ float2 sm[];
+    const int g = threadIdx.x / PL::T;
+    const int t = threadIdx.x - g * PL::T;
+    const int pulse = blockIdx.x * G + g;
+    const bool active = pulse < pulses;
+    float2* smg = sm + g * PL::smem_elems();
+    const float2* xr = x + (size_t)pulse * samples;
+    float2 v[PL::E];
+#pragma unroll
+    for (int r = 0; r < PL::E; ++r) {
+        const int e = t + PL::T * r;
+        v[r] = (active && e < samples) ? __ldcs(&xr[e]) : make_float2(0.f, 0.f);
+    }
+    fft_block<PL, -1, 1>(v, smg, t, tw);
+#pragma unroll
+    for (int r = 0; r < PL::E; ++r) v[r] = cmul(v[r], __ldg(&spectrum[t + PL::T * r]));
+    if constexpr (PL::PASSES > 1) __syncthreads();
+    fft_block<PL, 1, 1>(v, smg, t, tw);
+    if (active) {
+        float2* yr = y + (size_t)pulse * N;
+#pragma unroll
+        for (int r = 0; r < PL::E; ++r) __stcs(&yr[t + PL::T * r], v[r]);
+    }
+}
+
+// ------------------------------------------------------------------- Doppler
+
+// Range columns per Doppler CTA: 16 (128-byte row segments, conflict-free
+// interleave) while the CTA stays within 1024 threads, fewer for long transforms.
+constexpr int doppler_columns(int n)
+{
+    const int t = n / elems_for(n);
+    return t * 16 <= 1024 ? 16 : 1024 / t;
+}
+
+// CTA = C consecutive range columns x all pulses.  Thread (t, c) with c fastest, so
+// each warp touches C*8-byte row segments.  Columns are interleaved in shared memory
+// (element e of column c at e*C + c); with C = 16 every half-warp lands on distinct
+// banks without padding, smaller C uses the per-pass padding.
+template <int N>
+__global__ void __launch_bounds__(doppler_columns(N) * FftPlan<N, elems_for(N)>::T)
+pulse_doppler_kernel(const float2* __restrict__ x, int pulses, int samples,
+                     const float* __restrict__ window, float2* __restrict__ out,
+                     float* __restrict__ power, const float2* __restrict__ tw)
+{
+    using PL = FftPlan<N, elems_for(N)>;
+    constexpr int C = doppler_columns(N);
+    constexpr bool PAD = C < 16;
+    extern __shared__ float2 sm[];
+    const int c = threadIdx.x % C;
+    const int t = threadIdx.x / C;
+    const int col = blockIdx.x * C + c;
+    const bool active = col < samples;
+    (void)PAD;
+    float2 v[PL::E];
+#pragma unroll
+    for (int r = 0; r < PL::E; ++r) {
+        const int e = t + PL::T * r;
+        float2 a = make_float2(0.f, 0.f);
+        if (active && e < pulses) {
+            a = __ldcs(&x[(size_t)e * samples + col]);
+            if (window) {
+                const float w = __ldg(&window[e]);
+                a.x *= w;
+                a.y *= w;
+            }
+        }
+        v[r] = a;
+    }
+    fft_block<PL, -1, C, PAD>(v, sm + c, t, tw);
+    if (active) {
+#pragma unroll
+        for (int r = 0; r < PL::E; ++r) {
+            const size_t o = (size_t)(t + PL::T * r) * samples + col;
+            if (out) __stcs(&out[o], v[r]);
+            if (power) __stcs(&power[o], fmaf(v[r].x, v[r].x, v[r].y * v[r].y));
+        }
+    }
+}
+
+__global__ void doppler_window_kernel(int pulses, int kind, const float* explicit_window,
+                                      float* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < pulses) out[i] = window_value(kind, explicit_window, i, pulses);
+}
+
+// --------------------------------------------------------------- dispatchers
+
+template <int N>
+int replica_impl(const float2* h, int length, int normalize, int kind, const float* w,
+                 float2* spectrum, cudaStream_t s)
+{
+    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
+    using PL = FftPlan<N, elems_for(N)>;
+    const size_t smem = (size_t)PL::smem_elems() * sizeof(float2);
+    auto k = replica_spectrum_kernel<N>;
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<1, PL::T, smem, s>>>(h, length, normalize, kind, w, spectrum, twiddle_table());
+    ZKX_LAUNCHED("replica_spectrum_kernel");
+    return ZKX_SUCCESS;
+}
+
+template <int N>
+int compression_impl(const float2* x, int pulses, int samples, const float2* spectrum, float2* y,
+                     cudaStream_t s)
+{
+    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
+    using PL = FftPlan<N, elems_for(N)>;
+    constexpr int G = rows_per_cta(N);
+    const size_t smem = (size_t)G * PL::smem_elems() * sizeof(float2);
+    auto k = pulse_compression_kernel<N, G>;
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int blocks = (pulses + G - 1) / G;
+    k<<<blocks, G * PL::T, smem, s>>>(x, pulses, samples, spectrum, y, twiddle_table());
+    ZKX_LAUNCHED("pulse_compression_kernel");
+    return ZKX_SUCCESS;
+}
+
+template <int N>
+int doppler_impl(const float2* x, int pulses, int samples, const float* window, float2* out,
+                 float* power, cudaStream_t s)
+{
+    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
+    using PL = FftPlan<N, elems_for(N)>;
+    constexpr int C = doppler_columns(N);
+    const size_t smem = (size_t)C * PL::smem_elems(C < 16) * sizeof(float2);
+    if (smem > 227 * 1024) return fail(ZKX_UNSUPPORTED_OPERATION, "pulse_doppler: nfft above 4096 is not supported");
+    auto k = pulse_doppler_kernel<N>;
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int blocks = (samples + C - 1) / C;
+    k<<<blocks, C * PL::T, smem, s>>>(x, pulses, samples, window, out, power, twiddle_table());
+    ZKX_LAUNCHED("pulse_doppler_kernel");
+    return ZKX_SUCCESS;
+}
+
+#define ZKX_DISPATCH_POW2(LOG, CALL)                                                    \
+    switch (LOG) {                                                                      \
+    case 0: return CALL(1);     case 1: return CALL(2);     case 2: return CALL(4);     \
+    case 3: return CALL(8);     case 4: return CALL(16);    case 5: return CALL(32);    \
+    case 6: return CALL(64);    case 7: return CALL(128);   case 8: return CALL(256);   \
+    case 9: return CALL(512);   case 10: return CALL(1024); case 11: return CALL(2048); \
+    case 12: return CALL(4096); case 13: return CALL(8192); case 14: return CALL(16384);\
+    default: return fail(ZKX_UNSUPPORTED_OPERATION, "transform length above 16384");    \
+    }
+
+}  // namespace
+
+int launch_replica_spectrum(const float2* replica, int length, int nfft, int normalize,
+                            int window_kind, const float* explicit_window, float2* spectrum,
+                            cudaStream_t stream)
+{
+#define ZKX_CALL(NN) replica_impl<NN>(replica, length, normalize, window_kind, explicit_window, spectrum, stream)
+    ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
+#undef ZKX_CALL
+}
+
+int launch_pulse_compression(const float2* x, int pulses, int samples, int nfft,
+                             const float2* spectrum, float2* y, cudaStream_t stream)
+{
+#define ZKX_CALL(NN) compression_impl<NN>(x, pulses, samples, spectrum, y, stream)
+    ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
+#undef ZKX_CALL
+}
+
+int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft, const float* window,
+                         float2* out, float* power, cudaStream_t stream)
+{
+    if (nfft > 4096) return fail(ZKX_UNSUPPORTED_OPERATION, "pulse_doppler: nfft above 4096 is not supported");
+#define ZKX_CALL(NN) doppler_impl<NN>(x, pulses, samples, window, out, power, stream)
+    ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
+#undef ZKX_CALL
+}
+
+int launch_doppler_window(int pulses, int window_kind, const float* explicit_window, float* out,
+                          cudaStream_t stream)
+{
+    doppler_window_kernel<<<(pulses + 255) / 256, 256, 0, stream>>>(pulses, window_kind,
+                                                                    explicit_window, out);
+    ZKX_LAUNCHED("doppler_window_kernel");
+    return ZKX_SUCCESS;
+}
+
+}  // namespace zkx

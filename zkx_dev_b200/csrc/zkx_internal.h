@@ -1,0 +1,76 @@
+// Internal host-side helpers shared by the library's translation units: status
+// codes, the thread-local error message, CUDA error mapping and the per-device
+// initialisation (twiddle table, cached scratch buffers).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "../../include/zkx_rd.h"
+
+namespace zkx {
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_status(cudaError_t e, const char* what);
+
+// Throw-free wrappers: evaluate, map a CUDA failure to ZKX_CUDA_RUNTIME_ERROR or
+// ZKX_OUT_OF_MEMORY and return it from the enclosing function.
+#define ZKX_CUDA(call)                                              \
+    do {                                                            \
+        cudaError_t zkx_e_ = (call);                                \
+        if (zkx_e_ != cudaSuccess) return ::zkx::cuda_status(zkx_e_, #call); \
+    } while (0)
+#define ZKX_LAUNCHED(what)                                          \
+    do {                                                            \
+        cudaError_t zkx_e_ = cudaGetLastError();                    \
+        if (zkx_e_ != cudaSuccess) return ::zkx::cuda_status(zkx_e_, what); \
+    } while (0)
+#define ZKX_TRY(call)                                               \
+    do {                                                            \
+        int zkx_rc_ = (call);                                       \
+        if (zkx_rc_ != ZKX_SUCCESS) return zkx_rc_;                 \
+    } while (0)
+
+// Generate the FP64-accurate twiddle table on the current device (once).
+int ensure_device_ready();
+// Device address of the current device's twiddle table (after ensure_device_ready).
+const float2* twiddle_table();
+
+// Grow-only per-device scratch buffer identified by a slot number; the returned
+// pointer stays valid until the same slot is requested with a larger size on the
+// same device.  Callers on one device must order their use of a slot on one stream.
+enum ScratchSlot { kScratchReplica = 0, kScratchDopplerWindow = 1, kScratchCfarIntegral = 2,
+                   kScratchPolyTaps = 3, kScratchSlots = 4 };
+int scratch(ScratchSlot slot, std::size_t bytes, void** out);
+
+bool is_pow2(long long n);
+int ilog2_host(long long n);
+
+// Launchers implemented in the .cu files (all asynchronous on `stream`).
+int launch_replica_spectrum(const float2* replica, int length, int nfft, int normalize,
+                            int window_kind, const float* explicit_window, float2* spectrum,
+                            cudaStream_t stream);
+int launch_pulse_compression(const float2* x, int pulses, int samples, int nfft,
+                             const float2* spectrum, float2* y, cudaStream_t stream);
+int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft,
+                         const float* window, float2* out, float* power, cudaStream_t stream);
+int launch_doppler_window(int pulses, int window_kind, const float* explicit_window, float* out,
+                          cudaStream_t stream);
+int launch_ca_cfar_accurate(const float* x, int rows, int columns, int guard_rows,
+                            int guard_columns, int reference_rows, int reference_columns,
+                            double alpha, int reference_count, float* threshold,
+                            uint8_t* detections, cudaStream_t stream);
+int launch_ca_cfar_compat(const float* x, int rank, int rows, int columns, int guard_rows,
+                          int guard_columns, int reference_rows, int reference_columns,
+                          float alpha, int reference_count, float* cumulative, float* threshold,
+                          uint8_t* detections, cudaStream_t stream);
+int launch_fir(const float* b, int nb, const float* x, int lines, int n, const float* zi,
+               float* y, float* zf, cudaStream_t stream);
+int launch_polyphase(const float* taps, int ntaps, int up, int down, long long offset,
+                     const float* x, int lines, int n, float* y, int nout, cudaStream_t stream);
+
+}  // namespace zkx
