@@ -73,7 +73,7 @@ def _traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms in the background."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -89,7 +89,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, ValueError):
             self.proc = None
@@ -142,7 +142,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict:
     stream = torch.cuda.current_stream()
 
     # inputs: three rotating sets (host pinned + device copies)
-    n_sets = 3
+    n_sets = 1 if args.profile else 3
     host_fe, host_cube = [], []
     for i in range(n_sets):
         seed = synth.seed_for(2, rank * 100 + i)
@@ -191,6 +191,11 @@ def run_ours(args, rank: int, world: int, dist) -> dict:
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize()
+    if args.profile:
+        step(0)
+        torch.cuda.synchronize()
+        chain.close()
+        return None
 
     # per-stage timing (separate pass, kernels bracketed by events)
     stage_ms = {k: [] for k in ("fir", "resample_poly", "pulse_compression", "pulse_doppler", "ca_cfar")}
@@ -367,12 +372,15 @@ def reference_cpu_baseline(steps: int, warmup: int) -> dict:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="one input set, one warm-up and one step of every stage, no timing "
+                         "(the command profiled under ncu)")
     args = ap.parse_args()
-    args.warmup = max(3, args.warmup)
+    args.warmup = 1 if args.profile else max(3, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -406,6 +414,9 @@ def main() -> None:
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
     res = run_ours(args, rank, world, dist)
+    if res is None:
+        print("profile pass done")
+        return
     if rank == 0:
         line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],

@@ -112,3 +112,18 @@ def test_reference_design_matches_restatement(reference_lib):
     got, is64 = O.ref_resample_poly(x, 3, 2)
     assert is64
     np.testing.assert_array_equal(got, O.resample_poly(x, 3, 2))
+
+
+def test_reference_doppler_phase_error_grows_with_pulses():
+    """The reference's CPU pulse_doppler uses the float-rounded pi inside a double phase
+    (radartools_typed.cpp:14,742); the restatement reproduces it (pinned by the published
+    digests) and its distance to the exact DFT grows linearly with the pulse count."""
+    rng = np.random.default_rng(4)
+    errs = []
+    for P in (128, 512, 2048):
+        x = (rng.standard_normal((P, 8)) + 1j * rng.standard_normal((P, 8))).astype(np.complex64)
+        a = O.pulse_doppler_direct(x)
+        b, _ = O.pulse_doppler_fft64(x)
+        errs.append(np.linalg.norm(a - b) / np.linalg.norm(b))
+    assert 3e-6 < errs[0] < 1.5e-5
+    assert errs[2] > 8 * errs[0]

@@ -112,14 +112,26 @@ def test_pulse_compression_sampled_rows_vs_fp64_full_size(z):
                                       (2048, 16, -1), (512, 64, 256)])
 @pytest.mark.parametrize("window", ["none", "hamming"])
 def test_pulse_doppler_matches_reference(z, P, N, nfft, window):
+    """Against the exact FP64 DFT at 1e-5, and against the reference's own CPU function.
+    The reference evaluates the DFT phase in double but with the float-rounded pi
+    (radartools_typed.cpp:14,742), a phase error that grows with the pulse count
+    (7e-6 rel-L2 at 128 pulses, 1.2e-4 at 2048): up to 128 pulses the GPU must match it
+    within 1e-5; beyond, the GPU's distance to it may not exceed the reference's own
+    distance to the exact transform (plus 1e-6)."""
     rng = np.random.default_rng(P + N)
     x = cplx(rng, P, N)
     ref = O.pulse_doppler_direct(x, nfft, window)
+    w = O.radar_window_f32(window, P) if window != "none" else None
+    exact, _ = O.pulse_doppler_fft64(x, nfft, w)
     got, power = z.pulse_doppler(dev(x), window=None if window == "none" else window,
                                  nfft=None if nfft == -1 else nfft, return_power=True)
     got = got.cpu().numpy()
     assert got.shape == ref.shape
-    assert rel_l2(got, ref) <= REL_L2
+    assert rel_l2(got, exact) <= 2e-6
+    if P <= 128:
+        assert rel_l2(got, ref) <= REL_L2
+    else:
+        assert rel_l2(got, ref) <= rel_l2(ref, exact) + 1e-6
     assert rel_l2(power.cpu().numpy(), np.abs(got.astype(np.complex128)) ** 2) <= 1e-6
 
 
