@@ -70,6 +70,13 @@ enum {
 ZKX_API const char* zkx_last_error(void);
 ZKX_API const char* zkx_version(void);
 
+/* Device-side status of the library's kernels on the current device: waits for the
+ * device to go idle and reports in *code the first error a kernel recorded since the
+ * last clear (0 = none; 1 = a bulk-copy wait ran out of its ~1 s bound and the CTA
+ * left without computing).  clear != 0 resets the word.  No counterpart in the
+ * reference, whose kernels have no device-side waits. */
+ZKX_API int zkx_kernel_status(int clear, int* code);
+
 /* pulse_compression: y[p, :] = IFFT(FFT(x[p, :nfft]) * conj(FFT(w*h/||w*h||, nfft))).
  * Replaces cusignal::pulse_compression_device<float>
  * (include/cusignal/operators/radartools/radartools_typed.h:257-262; computation

@@ -286,3 +286,12 @@ def test_chain_config1_against_fp64(z):
     det = out["detections"].cpu().numpy()
     hits = sum(det[t.doppler_bin, t.delay] for t in cpi.targets if t.snr_db > 15)
     assert hits >= 0.8 * sum(1 for t in cpi.targets if t.snr_db > 15)
+
+
+def test_kernel_error_word_clear_after_parity_runs(z):
+    """No kernel recorded a bounded-wait timeout during the runs above."""
+    from zkx_dev_b200 import _lib
+    rng = np.random.default_rng(1)
+    x = dev(cplx(rng, 256, 1000))
+    z.pulse_doppler(x, window="hamming")
+    assert _lib.kernel_status(clear=True) == 0

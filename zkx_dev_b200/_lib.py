@@ -42,6 +42,7 @@ class RdDesc(ctypes.Structure):
 SIGNATURES = {
     "zkx_last_error": (ctypes.c_char_p, []),
     "zkx_version": (ctypes.c_char_p, []),
+    "zkx_kernel_status": (_I, [_I, ctypes.POINTER(_I)]),
     "zkx_pulse_compression_c64": (_I, [_P, _I, _I, _P, _I, _I, _I, _I, _P, _P, _P]),
     "zkx_replica_spectrum_c64": (_I, [_P, _I, _I, _I, _I, _P, _P, _P]),
     "zkx_pulse_compression_spectrum_c64": (_I, [_P, _I, _I, _I, _P, _P, _P]),
@@ -108,3 +109,10 @@ def stream_handle(stream=None) -> Optional[int]:
 
 def ptr(t) -> Optional[int]:
     return None if t is None else t.data_ptr()
+
+
+def kernel_status(clear: bool = True) -> int:
+    """Synchronise the device and return (and by default clear) the kernel error word."""
+    code = ctypes.c_int()
+    check(lib().zkx_kernel_status(int(clear), ctypes.byref(code)))
+    return code.value

@@ -1,6 +1,6 @@
 // 2-D cell-averaging CFAR for sm_100a, two modes.
 //
-// Accurate mode (the chain's default).  A CTA owns a 32 x 64 tile of cells and
+// Accurate mode (the chain's default).  A CTA owns a 64 x 64 tile of cells and
 // stages the tile plus its (guard + training) halo in shared memory once.  The
 // training-ring sum of a cell is assembled from separable pieces that are all sums
 // of non-negative terms (no outer-minus-inner cancellation):
@@ -27,7 +27,7 @@
 namespace zkx {
 namespace {
 
-constexpr int kCfarTY = 32;
+constexpr int kCfarTY = 64;
 constexpr int kCfarTX = 64;
 constexpr int kCfarThreads = 256;
 constexpr float kRecheckBand = 1e-5f;
@@ -64,63 +64,106 @@ cfar_accurate_kernel(const float* __restrict__ x, int rows, int cols, float scal
     constexpr int MR = GR + RR, MC = GC + RC;
     constexpr int TY = kCfarTY, TX = kCfarTX;
     constexpr int HR = TY + 2 * MR, HC = TX + 2 * MC;
-    constexpr int SAP = HC | 1;  // odd row pitch: a warp walking 32 rows hits 32 banks
-    __shared__ float P[HR][SAP];
-    __shared__ float SA[TY][SAP];
-    __shared__ float SB[TY][SAP];
+    constexpr int PITCH = HC | 1;  // odd row pitch: a warp walking 32 rows hits 32 banks
+    extern __shared__ float csm[];
+    float* P = csm;                       // [HR][PITCH] input tile with halo
+    float* SA = P + HR * PITCH;           // [TY][PITCH] training-row column sums
+    float* SB = SA + TY * PITCH;          // [TY][PITCH] guard-row column sums
     const int r0 = blockIdx.y * TY;
     const int c0 = blockIdx.x * TX;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int WARPS = kCfarThreads / 32;
 
-    for (int i = threadIdx.x; i < HR * HC; i += kCfarThreads) {
-        const int hr = i / HC, hc = i - hr * HC;
-        const int gr = r0 - MR + hr, gc = c0 - MC + hc;
-        P[hr][hc] = (gr >= 0 && gr < rows && gc >= 0 && gc < cols) ? __ldg(&x[(size_t)gr * cols + gc]) : 0.f;
+    // 1. halo tile: every thread issues all of its (float2 or scalar) loads before the
+    //    shared stores, so each SM keeps ~14 loads per thread in flight
+    const bool vec = ((MC & 1) == 0) && ((cols & 1) == 0) &&
+                     ((reinterpret_cast<uintptr_t>(x) & 7) == 0);
+    if (vec) {
+        constexpr int H2 = HC / 2;
+        constexpr int ITEMS = HR * H2;
+        constexpr int PER = (ITEMS + kCfarThreads - 1) / kCfarThreads;
+        float2 tmp[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            const int e = u * kCfarThreads + threadIdx.x;
+            const int hr = e / H2, h2 = e - hr * H2;
+            const int gr = r0 - MR + hr, gc = c0 - MC + 2 * h2;
+            float2 v = make_float2(0.f, 0.f);
+            if (e < ITEMS && gr >= 0 && gr < rows) {
+                const float* xrow = x + (size_t)gr * cols;
+                if (gc >= 0 && gc + 1 < cols) v = __ldg(reinterpret_cast<const float2*>(xrow + gc));
+                else {
+                    if (gc >= 0 && gc < cols) v.x = __ldg(xrow + gc);
+                    if (gc + 1 >= 0 && gc + 1 < cols) v.y = __ldg(xrow + gc + 1);
+                }
+            }
+            tmp[u] = v;
+        }
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            const int e = u * kCfarThreads + threadIdx.x;
+            if (e < ITEMS) {
+                const int hr = e / H2, h2 = e - hr * H2;
+                P[hr * PITCH + 2 * h2] = tmp[u].x;
+                P[hr * PITCH + 2 * h2 + 1] = tmp[u].y;
+            }
+        }
+    } else {
+        for (int hr = warp; hr < HR; hr += WARPS) {
+            const int gr = r0 - MR + hr;
+            for (int hc = lane; hc < HC; hc += 32) {
+                const int gc = c0 - MC + hc;
+                P[hr * PITCH + hc] = (gr >= 0 && gr < rows && gc >= 0 && gc < cols)
+                                         ? __ldg(x + (size_t)gr * cols + gc) : 0.f;
+            }
+        }
     }
     __syncthreads();
 
-    // vertical pieces: one thread per (halo column, 16-row segment)
+    // 2. vertical pieces: one thread per (halo column, 16-row segment)
     constexpr int SEG = 16;
     constexpr int VL = SEG + 2 * MR;
     for (int item = threadIdx.x; item < HC * (TY / SEG); item += kCfarThreads) {
-        const int hc = item % HC;
-        const int rb = (item / HC) * SEG;
+        const int seg = item / HC;
+        const int hc = item - seg * HC;
+        const int rb = seg * SEG;
         float v[VL];
 #pragma unroll
-        for (int i = 0; i < VL; ++i) v[i] = P[rb + i][hc];
+        for (int i = 0; i < VL; ++i) v[i] = P[(rb + i) * PITCH + hc];
         float wt[VL - RR + 1], wg[VL - 2 * GR];
         window_sums<RR, VL>(v, wt);
         window_sums<2 * GR + 1, VL>(v, wg);
 #pragma unroll
         for (int r = 0; r < SEG; ++r) {
-            SA[rb + r][hc] = wt[r] + wt[r + MR + GR + 1];
-            SB[rb + r][hc] = wg[r + MR - GR];
+            SA[(rb + r) * PITCH + hc] = wt[r] + wt[r + MR + GR + 1];
+            SB[(rb + r) * PITCH + hc] = wg[r + MR - GR];
         }
     }
     __syncthreads();
 
-    // horizontal: lane = row, warp = 8-column segment
-    constexpr int CS = TX / (kCfarThreads / TY);  // 8 columns per thread
+    // 3. horizontal: a warp walks 32 rows of one 16-column segment
+    constexpr int CS = 16;
     constexpr int HL = CS + 2 * MC;
     const int r = threadIdx.x % TY;
     const int cb = (threadIdx.x / TY) * CS;
+    const int grow = r0 + r;
+    if (grow >= rows) return;
     float a[HL], b[HL];
 #pragma unroll
     for (int i = 0; i < HL; ++i) {
-        a[i] = SA[r][cb + i];
-        b[i] = SB[r][cb + i];
+        a[i] = SA[r * PITCH + cb + i];
+        b[i] = SB[r * PITCH + cb + i];
     }
     float wa[HL - 2 * MC], wb[HL - RC + 1];
     window_sums<2 * MC + 1, HL>(a, wa);
     window_sums<RC, HL>(b, wb);
-    const int grow = r0 + r;
-    if (grow >= rows) return;
     const bool row_interior = grow >= MR && grow < rows - MR;
     float tout[CS];
     uint8_t dout[CS];
 #pragma unroll
     for (int j = 0; j < CS; ++j) {
         const int gcol = c0 + cb + j;
-        const float xv = P[r + MR][cb + j + MC];
+        const float xv = P[(r + MR) * PITCH + cb + j + MC];
         float t = 0.f;
         bool hit;
         if (row_interior && gcol >= MC && gcol < cols - MC) {
@@ -128,11 +171,12 @@ cfar_accurate_kernel(const float* __restrict__ x, int rows, int cols, float scal
             t = scale32 * ring;
             hit = xv > t;
             if (fabsf(xv - t) <= kRecheckBand * t) {
+                // re-decide in FP64 from the staged tile
                 double s = 0.0;
                 for (int dr = -MR; dr <= MR; ++dr)
                     for (int dc = -MC; dc <= MC; ++dc)
                         if (dr < -GR || dr > GR || dc < -GC || dc > GC)
-                            s += (double)P[r + MR + dr][cb + j + MC + dc];
+                            s += (double)P[(r + MR + dr) * PITCH + cb + j + MC + dc];
                 const double t64 = scale64 * s;
                 hit = (double)xv > t64;
                 t = (float)t64;
@@ -144,29 +188,32 @@ cfar_accurate_kernel(const float* __restrict__ x, int rows, int cols, float scal
         dout[j] = hit ? 1 : 0;
     }
     const int cstart = c0 + cb;
-    const bool thr_vec = ((reinterpret_cast<uintptr_t>(thr) & 15) == 0) && (cols & 3) == 0;
-    const bool det_vec = ((reinterpret_cast<uintptr_t>(det) & 7) == 0) && (cols & 7) == 0;
-    if (cstart + CS <= cols && thr_vec) {
-        float4* tp = reinterpret_cast<float4*>(thr + (size_t)grow * cols + cstart);
-        tp[0] = make_float4(tout[0], tout[1], tout[2], tout[3]);
-        tp[1] = make_float4(tout[4], tout[5], tout[6], tout[7]);
-        if (det_vec) {
-            uint2 packed;
-            packed.x = dout[0] | (dout[1] << 8) | (dout[2] << 16) | ((unsigned)dout[3] << 24);
-            packed.y = dout[4] | (dout[5] << 8) | (dout[6] << 16) | ((unsigned)dout[7] << 24);
-            *reinterpret_cast<uint2*>(det + (size_t)grow * cols + cstart) = packed;
-        } else {
+    float* trow = thr + (size_t)grow * cols + cstart;
+    uint8_t* drow = det + (size_t)grow * cols + cstart;
+    const bool full = cstart + CS <= cols;
+    if (full && ((reinterpret_cast<uintptr_t>(trow) & 15) == 0)) {
+        float4* tp = reinterpret_cast<float4*>(trow);
 #pragma unroll
-            for (int j = 0; j < CS; ++j) det[(size_t)grow * cols + cstart + j] = dout[j];
-        }
+        for (int q = 0; q < CS / 4; ++q)
+            tp[q] = make_float4(tout[4 * q], tout[4 * q + 1], tout[4 * q + 2], tout[4 * q + 3]);
     } else {
 #pragma unroll
-        for (int j = 0; j < CS; ++j) {
-            if (cstart + j < cols) {
-                thr[(size_t)grow * cols + cstart + j] = tout[j];
-                det[(size_t)grow * cols + cstart + j] = dout[j];
-            }
-        }
+        for (int j = 0; j < CS; ++j)
+            if (cstart + j < cols) trow[j] = tout[j];
+    }
+    if (full && ((reinterpret_cast<uintptr_t>(drow) & 15) == 0)) {
+        uint4 packed;
+        unsigned w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            w[q] = dout[4 * q] | (dout[4 * q + 1] << 8) | (dout[4 * q + 2] << 16) |
+                   ((unsigned)dout[4 * q + 3] << 24);
+        packed.x = w[0]; packed.y = w[1]; packed.z = w[2]; packed.w = w[3];
+        *reinterpret_cast<uint4*>(drow) = packed;
+    } else {
+#pragma unroll
+        for (int j = 0; j < CS; ++j)
+            if (cstart + j < cols) drow[j] = dout[j];
     }
 }
 
@@ -294,8 +341,13 @@ template <int GR, int GC, int RR, int RC>
 int accurate_impl(const float* x, int rows, int cols, float s32, double s64, float* thr,
                   uint8_t* det, cudaStream_t s)
 {
+    constexpr int HR = kCfarTY + 2 * (GR + RR), HC = kCfarTX + 2 * (GC + RC);
+    constexpr int PITCH = HC | 1;
+    const size_t smem = (size_t)(HR + 2 * kCfarTY) * PITCH * sizeof(float);
+    auto k = cfar_accurate_kernel<GR, GC, RR, RC>;
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((cols + kCfarTX - 1) / kCfarTX, (rows + kCfarTY - 1) / kCfarTY);
-    cfar_accurate_kernel<GR, GC, RR, RC><<<grid, kCfarThreads, 0, s>>>(x, rows, cols, s32, s64, thr, det);
+    k<<<grid, kCfarThreads, smem, s>>>(x, rows, cols, s32, s64, thr, det);
     ZKX_LAUNCHED("cfar_accurate_kernel");
     return ZKX_SUCCESS;
 }

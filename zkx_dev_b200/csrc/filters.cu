@@ -2,11 +2,10 @@
 // upfirdn / resample_poly, both along the last axis of row-major [lines, n] data.
 //
 // FIR: a CTA computes 4096 outputs of one line with 256 threads x 16 consecutive
-// outputs.  The input block plus its (nb - 1)-sample history and the taps are
-// staged in shared memory; every thread keeps a 16-value sliding window of inputs
-// in registers, so each tap costs one shared load, one broadcast tap load and 16
-// FMAs.  The staged input is skewed (one pad word per 16) so the 32 threads of a
-// warp, whose windows start 16 samples apart, read 32 different banks.
+// outputs.  The input block plus its history and the taps (zero-padded to a multiple
+// of 16) are staged in shared memory.  Per 16-tap chunk a thread loads the 16 taps
+// (4 broadcast 128-bit loads) and the 31 input samples its outputs touch (8 128-bit
+// loads) and performs 256 register FMAs: about 1.05 instructions per multiply-add.
 // Algorithmic traffic: 4 B in + 4 B out per sample; 2*nb FLOP per sample.
 //
 // Polyphase: output m uses phase ph = (m*down + offset) mod up and the taps
@@ -24,56 +23,91 @@ constexpr int kFirThreads = 256;
 constexpr int kFirPerThread = 16;
 constexpr int kFirBlock = kFirThreads * kFirPerThread;  // outputs per CTA
 
-__host__ __device__ __forceinline__ int fir_skew(int j) { return j + (j >> 4); }
+// Shared layout of the staged input: samples in 16-sample blocks, block b at word 20*b
+// (4 pad words per block), so the 128-bit loads of 8 threads whose windows start 16
+// samples apart land on 32 distinct banks.
+__host__ __device__ __forceinline__ int fir_block_word(int b) { return 20 * b; }
 
+// y[n0 + o + q] = sum_{k < nbp} b[k] x[n0 + o + q - k], o = 16*tid, q < 16, with the taps
+// zero-padded to nbp (a multiple of 16).  Relative sample index j = i - n0 + nbp - 1; for
+// tap chunk c the 31 samples a thread needs are blocks tid + nbp/16 - 1 - c and the next.
 __global__ void __launch_bounds__(kFirThreads)
-fir_kernel(const float* __restrict__ b, int nb, const float* __restrict__ x, int n,
+fir_kernel(const float* __restrict__ b, int nb, int nbp, const float* __restrict__ x, int n,
            const float* __restrict__ zi, float* __restrict__ y)
 {
-    extern __shared__ float sm[];
-    float* taps = sm;                       // nb
-    float* xs = sm + ((nb + 3) & ~3);       // skewed input, kFirBlock + nb - 1 samples
+    extern __shared__ __align__(16) float sm[];
+    float* taps = sm;                        // nbp
+    float* xs = sm + nbp;                    // skewed blocks
     const int line = blockIdx.y;
     const long long n0 = (long long)blockIdx.x * kFirBlock;
     const float* xl = x + (size_t)line * n;
-    const int hist = nb - 1;
-    for (int k = threadIdx.x; k < nb; k += kFirThreads) taps[k] = b[k];
-    const int span = kFirBlock + hist;
-    for (int j = threadIdx.x; j < span; j += kFirThreads) {
-        const long long src = n0 - hist + j;
-        xs[fir_skew(j)] = (src >= 0 && src < n) ? __ldcs(&xl[src]) : 0.f;
+    const int hist = nbp - 1;
+    for (int k = threadIdx.x; k < nbp; k += kFirThreads) taps[k] = k < nb ? b[k] : 0.f;
+    const int span = kFirBlock + hist;       // samples n0 - hist .. n0 + kFirBlock - 1
+    // 8 loads in flight per thread before their shared stores
+    for (int j0 = 0; j0 < span; j0 += 8 * kFirThreads) {
+        float tmp[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int j = j0 + u * kFirThreads + threadIdx.x;
+            const long long src = n0 - hist + j;
+            tmp[u] = (j < span && src >= 0 && src < n) ? __ldcs(&xl[src]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int j = j0 + u * kFirThreads + threadIdx.x;
+            if (j < span) xs[fir_block_word(j >> 4) + (j & 15)] = tmp[u];
+        }
     }
     __syncthreads();
 
-    // outputs n0 + o + q, q < 16, with o = 16 * tid; x[i - k] sits at xs[i - n0 + hist - k]
-    const int o = threadIdx.x * kFirPerThread;
     float acc[kFirPerThread];
-    float win[kFirPerThread];
 #pragma unroll
-    for (int q = 0; q < kFirPerThread; ++q) {
-        acc[q] = 0.f;
-        win[q] = xs[fir_skew(o + hist + q)];
-    }
-    // win[q] = x[n0 + o + q - k] at step k; unrolling by 16 turns the shifts into
-    // register renames
-#pragma unroll 16
-    for (int k = 0; k < nb; ++k) {
-        const float bk = taps[k];
+    for (int q = 0; q < kFirPerThread; ++q) acc[q] = 0.f;
+    const int chunks = nbp >> 4;
+    for (int c = 0; c < chunks; ++c) {
+        float bv[16];
+        const float4* tp = reinterpret_cast<const float4*>(taps + 16 * c);
 #pragma unroll
-        for (int q = 0; q < kFirPerThread; ++q) acc[q] = fmaf(bk, win[q], acc[q]);
+        for (int u = 0; u < 4; ++u) {
+            const float4 t4 = tp[u];
+            bv[4 * u] = t4.x; bv[4 * u + 1] = t4.y; bv[4 * u + 2] = t4.z; bv[4 * u + 3] = t4.w;
+        }
+        const int blk = threadIdx.x + chunks - 1 - c;
+        float xw[32];
+        const float4* w0 = reinterpret_cast<const float4*>(xs + fir_block_word(blk));
+        const float4* w1 = reinterpret_cast<const float4*>(xs + fir_block_word(blk + 1));
 #pragma unroll
-        for (int q = kFirPerThread - 1; q > 0; --q) win[q] = win[q - 1];
-        const int j = o + hist - k - 1;
-        win[0] = j >= 0 ? xs[fir_skew(j)] : 0.f;
+        for (int u = 0; u < 4; ++u) {
+            const float4 a = w0[u], d = w1[u];
+            xw[4 * u] = a.x; xw[4 * u + 1] = a.y; xw[4 * u + 2] = a.z; xw[4 * u + 3] = a.w;
+            xw[16 + 4 * u] = d.x; xw[17 + 4 * u] = d.y; xw[18 + 4 * u] = d.z; xw[19 + 4 * u] = d.w;
+        }
+        // tap 16c + kk on output q reads window position q - kk + 15
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+#pragma unroll
+            for (int q = 0; q < kFirPerThread; ++q) acc[q] = fmaf(bv[kk], xw[q - kk + 15], acc[q]);
+        }
     }
     float* yl = y + (size_t)line * n;
+    const int zhist = nb - 1;
+    const long long ob = n0 + threadIdx.x * kFirPerThread;
+    if (ob + kFirPerThread <= n && !(zi && ob < zhist) &&
+        ((reinterpret_cast<uintptr_t>(yl + ob) & 15) == 0)) {
+        float4* yp = reinterpret_cast<float4*>(yl + ob);
 #pragma unroll
-    for (int q = 0; q < kFirPerThread; ++q) {
-        const long long i = n0 + o + q;
-        if (i < n) {
-            float v = acc[q];
-            if (zi && i < hist) v += zi[(size_t)line * hist + i];
-            __stcs(&yl[i], v);
+        for (int u = 0; u < 4; ++u)
+            yp[u] = make_float4(acc[4 * u], acc[4 * u + 1], acc[4 * u + 2], acc[4 * u + 3]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < kFirPerThread; ++q) {
+            const long long i = ob + q;
+            if (i < n) {
+                float v = acc[q];
+                if (zi && i < zhist) v += zi[(size_t)line * zhist + i];
+                yl[i] = v;
+            }
         }
     }
 }
@@ -107,42 +141,156 @@ __device__ __forceinline__ long long floor_div(long long a, long long b)
 
 constexpr int kPolyThreads = 256;
 
+// Generic polyphase kernel: each thread walks Q consecutive outputs, tracking the
+// phase and input index incrementally in 32-bit arithmetic (one division per thread).
+template <int Q>
 __global__ void __launch_bounds__(kPolyThreads)
 polyphase_kernel(const float* __restrict__ h, int nh, int up, int down, long long offset,
-                 const float* __restrict__ x, int n, float* __restrict__ y, int nout, int block,
-                 int jmax, int span_cap)
+                 const float* __restrict__ x, int n, float* __restrict__ y, int nout, int jmax,
+                 int span_cap)
 {
     extern __shared__ float sm[];
     float* hp = sm;                               // [up][jmax] phase-major taps
     float* xs = sm + ((up * jmax + 3) & ~3);      // input span
+    constexpr int block = kPolyThreads * Q;
     const int line = blockIdx.y;
     const long long m0 = (long long)blockIdx.x * block;
-    const long long mlast = m0 + block - 1 < nout - 1 ? m0 + block - 1 : nout - 1;
-    const long long qlo = floor_div(m0 * down + offset, up) - (jmax - 1);
-    const long long qhi = floor_div(mlast * down + offset, up);
-    const int span = (int)(qhi - qlo + 1);
+    const long long base = m0 * down + offset;    // filter time of the CTA's first output
+    const long long qb = floor_div(base, up);
+    const int rb = (int)(base - qb * up);
+    const long long qlo = qb - (jmax - 1);
     const float* xl = x + (size_t)line * n;
     for (int i = threadIdx.x; i < up * jmax; i += kPolyThreads) {
-        const int ph = i / jmax, j = i % jmax;
+        const int ph = i / jmax, j = i - ph * jmax;
         const int k = ph + j * up;
         hp[i] = k < nh ? h[k] : 0.f;
     }
-    for (int i = threadIdx.x; i < span && i < span_cap; i += kPolyThreads) {
-        const long long s = qlo + i;
-        xs[i] = (s >= 0 && s < n) ? __ldcs(&xl[s]) : 0.f;
+    for (int i0 = 0; i0 < span_cap; i0 += 8 * kPolyThreads) {
+        float tmp[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + u * kPolyThreads + threadIdx.x;
+            const long long s = qlo + i;
+            tmp[u] = (i < span_cap && s >= 0 && s < n) ? __ldcs(&xl[s]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + u * kPolyThreads + threadIdx.x;
+            if (i < span_cap) xs[i] = tmp[u];
+        }
+    }
+    __syncthreads();
+    // first output of this thread: d = tid * Q, filter time rb + d * down (32-bit)
+    const int d0 = threadIdx.x * Q;
+    const int t0 = rb + d0 * down;
+    int q = t0 / up + (jmax - 1);                 // index into xs of the newest sample
+    int ph = t0 - (t0 / up) * up;
+    const int dq = down / up, dr = down - dq * up;
+    float* yl = y + (size_t)line * nout;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const long long m = m0 + d0 + i;
+        if (m < nout) {
+            const float* hrow = hp + ph * jmax;
+            float acc = 0.f;
+            for (int j = 0; j < jmax; ++j) acc = fmaf(hrow[j], xs[q - j], acc);
+            __stcs(&yl[m], acc);
+        }
+        ph += dr;
+        q += dq;
+        if (ph >= up) {
+            ph -= up;
+            ++q;
+        }
+    }
+}
+
+// Register-blocked polyphase for fixed (UP, DOWN, J): thread (g, r) computes the Q
+// outputs m = m0 + g*UP*Q + r + UP*i, which share one phase, so its J taps and the
+// J + DOWN*(Q-1) input samples they touch stay in registers (each sample is reused by
+// up to J/DOWN outputs).  Outputs are staged in shared memory and stored coalesced.
+template <int UP, int DOWN, int J, int Q>
+__global__ void __launch_bounds__((kPolyThreads / UP) * UP)
+polyphase_blocked_kernel(const float* __restrict__ h, int nh, long long offset,
+                         const float* __restrict__ x, int n, float* __restrict__ y, int nout,
+                         int span_cap)
+{
+    constexpr int G = kPolyThreads / UP;
+    constexpr int NT = G * UP;
+    constexpr int BLOCK = NT * Q;
+    constexpr int W = J + DOWN * (Q - 1);
+    extern __shared__ float sm[];
+    float* hp = sm;                              // [UP][J]
+    float* ys = hp + ((UP * J + 3) & ~3);        // BLOCK staged outputs
+    float* xs = ys + BLOCK;                      // input span
+    const int line = blockIdx.y;
+    const long long m0 = (long long)blockIdx.x * BLOCK;
+    const long long base = m0 * DOWN + offset;
+    const long long qb = floor_div(base, UP);
+    const int rb = (int)(base - qb * UP);
+    const long long qlo = qb - (J - 1);
+    const float* xl = x + (size_t)line * n;
+    for (int i = threadIdx.x; i < UP * J; i += NT) {
+        const int ph = i / J, j = i - ph * J;
+        const int k = ph + j * UP;
+        hp[i] = k < nh ? h[k] : 0.f;
+    }
+    for (int i0 = 0; i0 < span_cap; i0 += 8 * NT) {
+        float tmp[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + u * NT + threadIdx.x;
+            const long long s = qlo + i;
+            tmp[u] = (i < span_cap && s >= 0 && s < n) ? __ldcs(&xl[s]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + u * NT + threadIdx.x;
+            if (i < span_cap) xs[i] = tmp[u];
+        }
+    }
+    __syncthreads();
+    const int g = threadIdx.x / UP, r = threadIdx.x - (threadIdx.x / UP) * UP;
+    const int d0 = g * UP * Q + r;
+    const int t0 = rb + d0 * DOWN;
+    const int q0 = t0 / UP;                      // relative to qb
+    const int ph = t0 - q0 * UP;
+    float hreg[J];
+#pragma unroll
+    for (int j = 0; j < J; ++j) hreg[j] = hp[ph * J + j];
+    float xw[W];                                 // xw[w] = sample qb + q0 - (J-1) + w
+#pragma unroll
+    for (int w = 0; w < W; ++w) xw[w] = xs[q0 + w];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        float acc = 0.f;
+#pragma unroll
+        for (int j = 0; j < J; ++j) acc = fmaf(hreg[j], xw[J - 1 + DOWN * i - j], acc);
+        ys[d0 + UP * i] = acc;
     }
     __syncthreads();
     float* yl = y + (size_t)line * nout;
-    for (long long m = m0 + threadIdx.x; m <= mlast; m += kPolyThreads) {
-        const long long tt = m * down + offset;
-        const long long q = floor_div(tt, up);
-        const int ph = (int)(tt - q * up);
-        const float* hrow = hp + ph * jmax;
-        const int base = (int)(q - qlo);
-        float acc = 0.f;
-        for (int j = 0; j < jmax; ++j) acc = fmaf(hrow[j], xs[base - j], acc);
-        __stcs(&yl[m], acc);
+    for (int i = threadIdx.x; i < BLOCK; i += NT) {
+        const long long m = m0 + i;
+        if (m < nout) __stcs(&yl[m], ys[i]);
     }
+}
+
+template <int UP, int DOWN, int J, int Q>
+int polyphase_blocked_launch(const float* taps, int ntaps, long long offset, const float* x,
+                             int lines, int n, float* y, int nout, cudaStream_t stream)
+{
+    constexpr int NT = (kPolyThreads / UP) * UP;
+    constexpr int BLOCK = NT * Q;
+    // span: floor((BLOCK-1)*DOWN/UP) + 1 + J samples (+1 slack for the base remainder)
+    const int span_cap = (BLOCK * DOWN) / UP + J + 2;
+    const size_t smem = ((size_t)((UP * J + 3) & ~3) + BLOCK + span_cap) * sizeof(float);
+    auto k = polyphase_blocked_kernel<UP, DOWN, J, Q>;
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((unsigned)((nout + BLOCK - 1) / BLOCK), (unsigned)lines);
+    k<<<grid, NT, smem, stream>>>(taps, ntaps, offset, x, n, y, nout, span_cap);
+    ZKX_LAUNCHED("polyphase_blocked_kernel");
+    return ZKX_SUCCESS;
 }
 
 }  // namespace
@@ -151,12 +299,13 @@ int launch_fir(const float* b, int nb, const float* x, int lines, int n, const f
                float* y, float* zf, cudaStream_t stream)
 {
     if (lines > 65535) return fail(ZKX_UNSUPPORTED_OPERATION, "firfilter: more than 65535 lines");
-    const int span = kFirBlock + nb - 1;
-    const size_t smem = ((size_t)((nb + 3) & ~3) + (size_t)fir_skew(span) + 1) * sizeof(float);
+    const int nbp = (nb + 15) & ~15;
+    const int span = kFirBlock + nbp - 1;
+    const size_t smem = ((size_t)nbp + (size_t)fir_block_word((span + 15) >> 4)) * sizeof(float);
     if (smem > 200 * 1024) return fail(ZKX_UNSUPPORTED_OPERATION, "firfilter: too many taps for the shared-memory kernel");
     ZKX_CUDA(cudaFuncSetAttribute(fir_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)((n + kFirBlock - 1) / kFirBlock), (unsigned)lines);
-    fir_kernel<<<grid, kFirThreads, smem, stream>>>(b, nb, x, n, zi, y);
+    fir_kernel<<<grid, kFirThreads, smem, stream>>>(b, nb, nbp, x, n, zi, y);
     ZKX_LAUNCHED("fir_kernel");
     if (zf && nb > 1) {
         const long long total = (long long)lines * (nb - 1);
@@ -172,16 +321,24 @@ int launch_polyphase(const float* taps, int ntaps, int up, int down, long long o
     if (nout <= 0 || lines <= 0) return ZKX_SUCCESS;
     if (lines > 65535) return fail(ZKX_UNSUPPORTED_OPERATION, "upfirdn: more than 65535 lines");
     const int jmax = (ntaps + up - 1) / up;
-    // outputs per CTA: keep the staged input span within 12K samples
-    long long block = 2048;
-    while (block > kPolyThreads && (block * down) / up + jmax + 2 > 12288) block /= 2;
-    const int span_cap = (int)((block * down) / up + jmax + 2);
+    // register-blocked kernels for the common rational factors with designed filters
+    if (up == 3 && down == 2 && jmax == 21) return polyphase_blocked_launch<3, 2, 21, 7>(taps, ntaps, offset, x, lines, n, y, nout, stream);
+    if (up == 2 && down == 1 && jmax == 21) return polyphase_blocked_launch<2, 1, 21, 8>(taps, ntaps, offset, x, lines, n, y, nout, stream);
+    if (up == 2 && down == 3 && jmax == 31) return polyphase_blocked_launch<2, 3, 31, 5>(taps, ntaps, offset, x, lines, n, y, nout, stream);
+    if (up == 1 && down == 2 && jmax == 41) return polyphase_blocked_launch<1, 2, 41, 4>(taps, ntaps, offset, x, lines, n, y, nout, stream);
+    constexpr int Q = 8;
+    constexpr long long block = (long long)kPolyThreads * Q;
+    // span: floor((block-1)*down/up) + 1 + jmax samples, plus slack for the remainder
+    const long long span_ll = (block * down) / up + jmax + 2;
+    if (up > 4096 || down > 4096 || span_ll > 48 * 1024)
+        return fail(ZKX_UNSUPPORTED_OPERATION, "upfirdn: factors too large for the shared-memory kernel");
+    const int span_cap = (int)span_ll;
     const size_t smem = ((size_t)((up * jmax + 3) & ~3) + (size_t)span_cap) * sizeof(float);
     if (smem > 200 * 1024) return fail(ZKX_UNSUPPORTED_OPERATION, "upfirdn: filter too long for the shared-memory kernel");
-    ZKX_CUDA(cudaFuncSetAttribute(polyphase_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ZKX_CUDA(cudaFuncSetAttribute(polyphase_kernel<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)((nout + block - 1) / block), (unsigned)lines);
-    polyphase_kernel<<<grid, kPolyThreads, smem, stream>>>(taps, ntaps, up, down, offset, x, n, y,
-                                                           nout, (int)block, jmax, span_cap);
+    polyphase_kernel<Q><<<grid, kPolyThreads, smem, stream>>>(taps, ntaps, up, down, offset, x, n, y,
+                                                             nout, jmax, span_cap);
     ZKX_LAUNCHED("polyphase_kernel");
     return ZKX_SUCCESS;
 }

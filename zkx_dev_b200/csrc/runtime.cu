@@ -1,7 +1,10 @@
 // Library runtime: error reporting, per-device initialisation (FP64-generated
 // twiddle table) and grow-only per-device scratch buffers.
 #include "fft_core.cuh"
+#include "tma.cuh"
 #include "zkx_internal.h"
+
+#include <cudaTypedefs.h>
 
 #include <mutex>
 #include <string>
@@ -11,6 +14,7 @@ namespace zkx {
 
 namespace {
 __device__ float2 g_twiddle[kTwiddleSize];
+__device__ int g_kernel_error;
 
 thread_local std::string g_error;
 
@@ -28,6 +32,9 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
 bool g_ready[kMaxDevices] = {};
 const float2* g_table[kMaxDevices] = {};
+int* g_error_word[kMaxDevices] = {};
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::once_flag g_encode_once;
 struct ScratchEntry {
     void* ptr = nullptr;
     std::size_t bytes = 0;
@@ -76,9 +83,40 @@ int ensure_device_ready()
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
     if (e != cudaSuccess) return cuda_status(e, "twiddle table initialisation");
+    int* word = nullptr;
+    ZKX_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&word), g_kernel_error));
+    ZKX_CUDA(cudaMemset(word, 0, sizeof(int)));
+    g_error_word[dev] = word;
     g_table[dev] = table;
     g_ready[dev] = true;
     return ZKX_SUCCESS;
+}
+
+int* kernel_error_word()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    return g_error_word[dev];
+}
+
+bool encode_tensor_map_2d_f32(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
+                              uint64_t row_pitch_bytes, uint32_t box_inner, uint32_t box_outer)
+{
+    std::call_once(g_encode_once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    if (!g_encode) return false;
+    const cuuint64_t dims[2] = {inner, outer};
+    const cuuint64_t strides[1] = {row_pitch_bytes};
+    const cuuint32_t box[2] = {box_inner, box_outer};
+    const cuuint32_t estr[2] = {1, 1};
+    return g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides,
+                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 const float2* twiddle_table()
@@ -113,4 +151,16 @@ int scratch(ScratchSlot slot, std::size_t bytes, void** out)
 }  // namespace zkx
 
 extern "C" const char* zkx_last_error(void) { return zkx::g_error.c_str(); }
+
+extern "C" int zkx_kernel_status(int clear, int* code)
+{
+    using namespace zkx;
+    if (!code) return fail(ZKX_INVALID_ARGUMENT, "kernel_status: null pointer");
+    ZKX_TRY(ensure_device_ready());
+    int* word = kernel_error_word();
+    ZKX_CUDA(cudaDeviceSynchronize());
+    ZKX_CUDA(cudaMemcpy(code, word, sizeof(int), cudaMemcpyDeviceToHost));
+    if (clear) ZKX_CUDA(cudaMemset(word, 0, sizeof(int)));
+    return ZKX_SUCCESS;
+}
 extern "C" const char* zkx_version(void) { return "zkx_rd 0.1.0 (sm_100a)"; }

@@ -39,6 +39,8 @@ int cuda_status(cudaError_t e, const char* what);
 int ensure_device_ready();
 // Device address of the current device's twiddle table (after ensure_device_ready).
 const float2* twiddle_table();
+// Device address of the current device's kernel error word (after ensure_device_ready).
+int* kernel_error_word();
 
 // Grow-only per-device scratch buffer identified by a slot number; the returned
 // pointer stays valid until the same slot is requested with a larger size on the
