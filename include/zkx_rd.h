@@ -90,6 +90,24 @@ ZKX_API int zkx_pulse_compression_c64(const void* x, int num_pulses, int samples
                               int window_kind, const float* explicit_window, void* y,
                               zkx_stream_t stream);
 
+/* pulse_compression that allocates no device memory, for callers that cannot let a
+ * library allocate: processing loops that must not call cudaMalloc/cudaFree once they
+ * run (those calls can block and synchronise the device) and hosts whose device
+ * memory is owned by another allocator or a fixed budget.  Same arguments and result
+ * as zkx_pulse_compression_c64 (the caller passes inputs and outputs); the replica
+ * spectrum goes to a file-scope device array of 16384 complex64 (128 KiB) that every
+ * GPU loading the library holds until the process exits.  nfft above 16384 is
+ * rejected with ZKX_INVALID_ARGUMENT.  The first call on a device initialises the
+ * library's twiddle table there (a synchronous set-up) and looks up the array's
+ * device address, so make that first call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU (other streams or host threads) race.
+ * No counterpart in the reference. */
+ZKX_API int zkx_pulse_compression_c64_noalloc(const void* x, int num_pulses, int samples_per_pulse,
+                                              const void* replica, int replica_length, int nfft,
+                                              int normalize, int window_kind,
+                                              const float* explicit_window, void* y,
+                                              zkx_stream_t stream);
+
 /* The replica spectrum alone: spectrum[k] = conj(FFT(w*h/||w*h||, nfft))[k] / nfft,
  * the per-bin factor that zkx_pulse_compression_spectrum_c64 applies.  Lets callers
  * keep a spectrum resident per waveform (no counterpart call in the reference, which

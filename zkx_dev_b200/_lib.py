@@ -44,6 +44,7 @@ SIGNATURES = {
     "zkx_version": (ctypes.c_char_p, []),
     "zkx_kernel_status": (_I, [_I, ctypes.POINTER(_I)]),
     "zkx_pulse_compression_c64": (_I, [_P, _I, _I, _P, _I, _I, _I, _I, _P, _P, _P]),
+    "zkx_pulse_compression_c64_noalloc": (_I, [_P, _I, _I, _P, _I, _I, _I, _I, _P, _P, _P]),
     "zkx_replica_spectrum_c64": (_I, [_P, _I, _I, _I, _I, _P, _P, _P]),
     "zkx_pulse_compression_spectrum_c64": (_I, [_P, _I, _I, _I, _P, _P, _P]),
     "zkx_pulse_doppler_c64": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, _P]),
