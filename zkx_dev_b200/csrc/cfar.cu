@@ -22,6 +22,7 @@
 // Algorithmic HBM traffic of the accurate kernel: 4 B read + 4 B threshold + 1 B
 // mask = 9 B per cell.
 #include "fft_core.cuh"
+#include "tma.cuh"
 #include "zkx_internal.h"
 
 namespace zkx {
@@ -217,6 +218,155 @@ cfar_accurate_kernel(const float* __restrict__ x, int rows, int cols, float scal
     }
 }
 
+// TMA variant of the accurate kernel: the halo tile arrives as one 2-D bulk copy (box
+// of BOXW x HR floats starting OFF columns left of the halo, so its x coordinate is a
+// 16-byte multiple; rows and columns outside the image are zero-filled by the copy
+// engine), which leaves the threads only the arithmetic.
+template <int GR, int GC, int RR, int RC>
+struct CfarTmaGeom {
+    static constexpr int MR = GR + RR, MC = GC + RC;
+    static constexpr int HR = kCfarTY + 2 * MR, HC = kCfarTX + 2 * MC;
+    static constexpr int OFF = ((MC + 3) & ~3) - MC;       // leading pad columns
+    static constexpr int BOXW = (HC + OFF + 3) & ~3;        // box width (floats)
+    static constexpr int PITCH = HC | 1;                    // SA/SB pitch
+    static constexpr size_t smem_bytes()
+    {
+        return (size_t)HR * BOXW * sizeof(float) + (size_t)2 * kCfarTY * PITCH * sizeof(float) + 16;
+    }
+};
+
+template <int GR, int GC, int RR, int RC>
+__global__ void __launch_bounds__(kCfarThreads, 3)
+cfar_accurate_tma_kernel(const __grid_constant__ CUtensorMap tmap, int rows, int cols,
+                         float scale32, double scale64, float* __restrict__ thr,
+                         uint8_t* __restrict__ det, int* err)
+{
+    using G = CfarTmaGeom<GR, GC, RR, RC>;
+    constexpr int MR = G::MR, MC = G::MC, HC = G::HC, OFF = G::OFF, BOXW = G::BOXW;
+    constexpr int PITCH = G::PITCH, TY = kCfarTY, TX = kCfarTX;
+    extern __shared__ __align__(128) float csm[];
+    float* P = csm;                           // [HR][BOXW]; halo column hc at P[.. + hc + OFF]
+    float* SA = P + G::HR * BOXW;             // [TY][PITCH]
+    float* SB = SA + TY * PITCH;              // [TY][PITCH]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(SB + TY * PITCH);
+    const int r0 = blockIdx.y * TY;
+    const int c0 = blockIdx.x * TX;
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(bar, (uint32_t)(G::HR * BOXW * sizeof(float)));
+        tma_load_2d(P, &tmap, c0 - MC - OFF, r0 - MR, bar);
+    }
+    const bool ok = mbar_wait_bounded(bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
+        return;
+    }
+
+    constexpr int SEG = 16;
+    constexpr int VL = SEG + 2 * MR;
+    for (int item = threadIdx.x; item < HC * (TY / SEG); item += kCfarThreads) {
+        const int seg = item / HC;
+        const int hc = item - seg * HC;
+        const int rb = seg * SEG;
+        float v[VL];
+#pragma unroll
+        for (int i = 0; i < VL; ++i) v[i] = P[(rb + i) * BOXW + hc + OFF];
+        float wt[VL - RR + 1], wg[VL - 2 * GR];
+        window_sums<RR, VL>(v, wt);
+        window_sums<2 * GR + 1, VL>(v, wg);
+#pragma unroll
+        for (int r = 0; r < SEG; ++r) {
+            SA[(rb + r) * PITCH + hc] = wt[r] + wt[r + MR + GR + 1];
+            SB[(rb + r) * PITCH + hc] = wg[r + MR - GR];
+        }
+    }
+    __syncthreads();
+
+    constexpr int CS = 16;
+    constexpr int HL = CS + 2 * MC;
+    const int r = threadIdx.x % TY;
+    const int cb = (threadIdx.x / TY) * CS;
+    const int grow = r0 + r;
+    if (grow >= rows) return;
+    float a[HL], b[HL];
+#pragma unroll
+    for (int i = 0; i < HL; ++i) {
+        a[i] = SA[r * PITCH + cb + i];
+        b[i] = SB[r * PITCH + cb + i];
+    }
+    float wa[HL - 2 * MC], wb[HL - RC + 1];
+    window_sums<2 * MC + 1, HL>(a, wa);
+    window_sums<RC, HL>(b, wb);
+    // cell values: columns cb..cb+15 of tile row r (aligned 128-bit loads when possible)
+    float xv[CS];
+    const float* prow = P + (r + MR) * BOXW + cb + MC + OFF;
+    if constexpr (((MC + OFF) & 3) == 0 && (BOXW & 3) == 0) {
+#pragma unroll
+        for (int q = 0; q < CS / 4; ++q) {
+            const float4 f = reinterpret_cast<const float4*>(prow)[q];
+            xv[4 * q] = f.x; xv[4 * q + 1] = f.y; xv[4 * q + 2] = f.z; xv[4 * q + 3] = f.w;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < CS; ++j) xv[j] = prow[j];
+    }
+    const bool row_interior = grow >= MR && grow < rows - MR;
+    float tout[CS];
+    uint8_t dout[CS];
+#pragma unroll
+    for (int j = 0; j < CS; ++j) {
+        const int gcol = c0 + cb + j;
+        float t = 0.f;
+        bool hit;
+        if (row_interior && gcol >= MC && gcol < cols - MC) {
+            const float ring = wa[j] + (wb[j] + wb[j + MC + GC + 1]);
+            t = scale32 * ring;
+            hit = xv[j] > t;
+            if (fabsf(xv[j] - t) <= kRecheckBand * t) {
+                double s = 0.0;
+                for (int dr = -MR; dr <= MR; ++dr)
+                    for (int dc = -MC; dc <= MC; ++dc)
+                        if (dr < -GR || dr > GR || dc < -GC || dc > GC)
+                            s += (double)P[(r + MR + dr) * BOXW + cb + j + MC + OFF + dc];
+                const double t64 = scale64 * s;
+                hit = (double)xv[j] > t64;
+                t = (float)t64;
+            }
+        } else {
+            hit = xv[j] > 0.f;
+        }
+        tout[j] = t;
+        dout[j] = hit ? 1 : 0;
+    }
+    const int cstart = c0 + cb;
+    float* trow = thr + (size_t)grow * cols + cstart;
+    uint8_t* drow = det + (size_t)grow * cols + cstart;
+    const bool full = cstart + CS <= cols;
+    if (full && ((reinterpret_cast<uintptr_t>(trow) & 15) == 0)) {
+        float4* tp = reinterpret_cast<float4*>(trow);
+#pragma unroll
+        for (int q = 0; q < CS / 4; ++q)
+            tp[q] = make_float4(tout[4 * q], tout[4 * q + 1], tout[4 * q + 2], tout[4 * q + 3]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < CS; ++j)
+            if (cstart + j < cols) trow[j] = tout[j];
+    }
+    if (full && ((reinterpret_cast<uintptr_t>(drow) & 15) == 0)) {
+        unsigned w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            w[q] = dout[4 * q] | (dout[4 * q + 1] << 8) | (dout[4 * q + 2] << 16) |
+                   ((unsigned)dout[4 * q + 3] << 24);
+        *reinterpret_cast<uint4*>(drow) = make_uint4(w[0], w[1], w[2], w[3]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < CS; ++j)
+            if (cstart + j < cols) drow[j] = dout[j];
+    }
+}
+
 // Any window geometry: one thread per cell, ring summed directly in FP64.
 __global__ void cfar_generic_kernel(const float* __restrict__ x, int rows, int cols, int gr, int gc,
                                     int rr, int rc, double scale64, float* __restrict__ thr,
@@ -341,12 +491,25 @@ template <int GR, int GC, int RR, int RC>
 int accurate_impl(const float* x, int rows, int cols, float s32, double s64, float* thr,
                   uint8_t* det, cudaStream_t s)
 {
+    dim3 grid((cols + kCfarTX - 1) / kCfarTX, (rows + kCfarTY - 1) / kCfarTY);
+    using G = CfarTmaGeom<GR, GC, RR, RC>;
+    if ((cols & 3) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+        CUtensorMap map;
+        if (encode_tensor_map_2d_f32(&map, x, (uint64_t)cols, (uint64_t)rows,
+                                     (uint64_t)cols * sizeof(float), G::BOXW, G::HR)) {
+            const size_t smem = G::smem_bytes();
+            auto k = cfar_accurate_tma_kernel<GR, GC, RR, RC>;
+            ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k<<<grid, kCfarThreads, smem, s>>>(map, rows, cols, s32, s64, thr, det, kernel_error_word());
+            ZKX_LAUNCHED("cfar_accurate_tma_kernel");
+            return ZKX_SUCCESS;
+        }
+    }
     constexpr int HR = kCfarTY + 2 * (GR + RR), HC = kCfarTX + 2 * (GC + RC);
     constexpr int PITCH = HC | 1;
     const size_t smem = (size_t)(HR + 2 * kCfarTY) * PITCH * sizeof(float);
     auto k = cfar_accurate_kernel<GR, GC, RR, RC>;
     ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((cols + kCfarTX - 1) / kCfarTX, (rows + kCfarTY - 1) / kCfarTY);
     k<<<grid, kCfarThreads, smem, s>>>(x, rows, cols, s32, s64, thr, det);
     ZKX_LAUNCHED("cfar_accurate_kernel");
     return ZKX_SUCCESS;

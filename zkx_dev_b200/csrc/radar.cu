@@ -9,6 +9,8 @@
 // Range compression reads each pulse once and writes it once: 16 B per cell of
 // compulsory HBM traffic.  The Doppler kernel reads the compressed cube once and
 // writes the map (8 B) and the power (4 B): 20 B per cell.
+#include <algorithm>
+
 #include "fft_core.cuh"
 #include "tma.cuh"
 #include "zkx_internal.h"
@@ -18,10 +20,13 @@ namespace {
 
 // Values per thread for a transform of length N (a plan table chosen so that every
 // pass but the last uses the full radix and the thread count stays in 8..512).
+#ifndef ZKX_E16384
+#define ZKX_E16384 32
+#endif
 constexpr int elems_for(int n)
 {
     return n <= 32 ? n : n == 64 ? 8 : n == 128 ? 16 : n == 256 ? 16 : n == 512 ? 32
-         : n == 1024 ? 32 : n == 2048 ? 16 : n == 4096 ? 16 : 32;
+         : n == 1024 ? 32 : n == 2048 ? 16 : n == 4096 ? 16 : n == 8192 ? 32 : ZKX_E16384;
 }
 
 // Transforms per CTA for row kernels: aim for >= 128 threads per CTA.
@@ -125,6 +130,69 @@ pulse_compression_kernel(const float2* __restrict__ x, int pulses, int samples,
     if constexpr (PL::PASSES > 1) __syncthreads();
     fft_block<PL, 1, 1>(v, smg, t, tw);
     if (active) {
+        float2* yr = y + (size_t)pulse * N;
+#pragma unroll
+        for (int r = 0; r < PL::E; ++r) yr[t + PL::T * r] = v[r];  // stays in L2 for the next stage
+    }
+}
+
+// Persistent variant for long pulses (one 512-thread CTA per SM holds a whole
+// transform in shared memory, so CTAs cannot overlap each other's memory phases).
+// Each CTA walks pulses blockIdx.x, +gridDim.x, ...; as soon as the inverse transform
+// of one pulse has read the exchange buffer for the last time, one thread issues bulk
+// copies of the CTA's next pulse into that buffer, so the load streams in while the
+// current results are being stored.  Pulses are read from the staged copy
+// (unpadded, element e at sm[e]), zero beyond `samples`.
+template <int N>
+__global__ void __launch_bounds__(FftPlan<N, elems_for(N)>::T)
+pulse_compression_persistent_kernel(const float2* __restrict__ x, int pulses, int samples,
+                                    const float2* __restrict__ spectrum, float2* __restrict__ y,
+                                    const float2* __restrict__ tw, int* err)
+{
+    using PL = FftPlan<N, elems_for(N)>;
+    extern __shared__ __align__(128) float2 sm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + PL::smem_elems());
+    const int t = threadIdx.x;
+    const int copy = samples < N ? samples : N;                 // elements staged per pulse
+    const uint32_t bytes = (uint32_t)copy * (uint32_t)sizeof(float2);
+    constexpr uint32_t kChunk = 32768;                          // bytes per bulk copy
+    auto issue = [&](int pulse) {
+        mbar_arrive_expect_tx(bar, bytes);
+        const char* src = reinterpret_cast<const char*>(x + (size_t)pulse * samples);
+        char* dst = reinterpret_cast<char*>(sm);
+        for (uint32_t off = 0; off < bytes; off += kChunk)
+            bulk_load_1d(dst + off, src + off, bytes - off < kChunk ? bytes - off : kChunk, bar);
+    };
+    if (t == 0) mbar_init(bar, 1);
+    __syncthreads();
+    int pulse = blockIdx.x;
+    if (t == 0 && pulse < pulses) issue(pulse);
+    uint32_t phase = 0;
+    for (; pulse < pulses; pulse += gridDim.x) {
+        const bool ok = mbar_wait_bounded(bar, phase);
+        if (__syncthreads_or(!ok)) {
+            if (t == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
+            return;
+        }
+        phase ^= 1u;
+        float2 v[PL::E];
+#pragma unroll
+        for (int r = 0; r < PL::E; ++r) {
+            const int e = t + PL::T * r;
+            v[r] = e < copy ? sm[e] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        fft_block<PL, -1, 1>(v, sm, t, tw);
+#pragma unroll
+        for (int r = 0; r < PL::E; ++r) v[r] = cmul(v[r], __ldg(&spectrum[t + PL::T * r]));
+        __syncthreads();
+        fft_block<PL, 1, 1>(v, sm, t, tw);
+        // every thread is done with the exchange buffer; order those accesses before the
+        // bulk copy that overwrites it
+        fence_proxy_async_smem();
+        __syncthreads();
+        const int next = pulse + gridDim.x;
+        if (t == 0 && next < pulses) issue(next);
         float2* yr = y + (size_t)pulse * N;
 #pragma unroll
         for (int r = 0; r < PL::E; ++r) yr[t + PL::T * r] = v[r];  // stays in L2 for the next stage
@@ -277,6 +345,24 @@ int compression_impl(const float2* x, int pulses, int samples, const float2* spe
 {
     if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
     using PL = FftPlan<N, elems_for(N)>;
+    if constexpr (N >= 4096) {
+        // persistent bulk-copy pipeline: 16-byte aligned pulses (even length, aligned base)
+        if ((samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+            int dev = 0, sms = 0;
+            ZKX_CUDA(cudaGetDevice(&dev));
+            ZKX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            const size_t smem = (size_t)PL::smem_elems() * sizeof(float2) + 16;
+            auto k = pulse_compression_persistent_kernel<N>;
+            ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int per_sm = 0;
+            ZKX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, PL::T, smem));
+            const int grid = std::max(1, std::min(pulses, sms * std::max(per_sm, 1)));
+            k<<<grid, PL::T, smem, s>>>(x, pulses, samples, spectrum, y, twiddle_table(),
+                                        kernel_error_word());
+            ZKX_LAUNCHED("pulse_compression_persistent_kernel");
+            return ZKX_SUCCESS;
+        }
+    }
     constexpr int G = rows_per_cta(N);
     const size_t smem = (size_t)G * PL::smem_elems() * sizeof(float2);
     auto k = pulse_compression_kernel<N, G>;

@@ -65,6 +65,23 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
+// 1-D bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) into
+// shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Orders this thread's earlier generic-proxy shared-memory accesses before later
+// async-proxy (bulk copy) writes to the same memory.
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // Host: encode a row-major 2-D FP32 tensor [outer, inner] with the given row pitch
 // (bytes, a multiple of 16) and box (inner x outer elements).  Returns false when the
 // driver entry point is unavailable or the encoding is rejected.
