@@ -1,0 +1,278 @@
+// cusignal_cpp radar tools on the range-Doppler chain -- pulse_compression,
+// pulse_doppler, ca_cfar, cfar_alpha -- with the signatures of
+// ZKX/cusignal_cpp/include/cusignal/operators/radartools/radartools_typed.h (39-94,
+// 154-311), implemented over libzkx_rd.so on the legacy default stream.  T is one of
+// float, __half, int32_t, int16_t, int8_t (converted to FP32 on the device first).
+// Results follow the reference's dtype rules: complex results are FP32 unless a window
+// is used or T is an integer, in which case the FP32 result is widened exactly into FP64
+// storage; CA-CFAR returns FP32 thresholds and one-byte detections computed with the
+// reference's FP32 integral-image order (bit-identical to ca_cfar_typed_cpu<float>).
+// The *_typed_cpu CPU references keep their declarations for callers that link the
+// reference's own CPU implementation.
+#pragma once
+
+#include <cusignal/operators/filtering/filtering_typed.h>
+
+#include <cmath>
+#include <cstdint>
+#include <limits>
+#include <stdexcept>
+#include <type_traits>
+#include <vector>
+
+namespace cusignal {
+
+enum class CfarDetection : std::uint8_t { no = 0, yes = 1 };
+
+struct CaCfarOptions {
+    std::vector<int> guard_cells;
+    std::vector<int> reference_cells;
+    double pfa = 1.0e-3;
+};
+
+struct CaCfarCpuResult {
+    std::vector<float> threshold;
+    std::vector<CfarDetection> detections;
+    std::vector<int> shape;
+};
+
+struct CaCfarDeviceResult {
+    DeviceArray<float> threshold;
+    DeviceArray<CfarDetection> detections;
+    std::vector<int> shape;
+};
+
+enum class RadarWindowKind { none, hann, hamming, explicit_fp32, explicit_fp64 };
+
+struct PulseCompressionOptions {
+    int num_pulses{0};
+    int samples_per_pulse{0};
+    bool normalize{false};
+    int nfft{-1};
+    RadarWindowKind window{RadarWindowKind::none};
+};
+
+struct PulseDopplerOptions {
+    int num_pulses{0};
+    int samples_per_pulse{0};
+    int nfft{-1};
+    RadarWindowKind window{RadarWindowKind::none};
+};
+
+struct RadarComplexCpuResult {
+    std::vector<ComplexFloat> fp32;
+    std::vector<ComplexDouble> fp64;
+    std::vector<int> shape;
+    bool is_fp64{false};
+};
+
+struct RadarComplexDeviceResult {
+    DeviceArray<ComplexFloat> fp32;
+    DeviceArray<ComplexDouble> fp64;
+    std::vector<int> shape;
+    bool is_fp64{false};
+};
+
+namespace detail {
+
+// radartools_typed.cpp:271-278
+template <class T>
+bool radar_result_is_fp64(RadarWindowKind window)
+{
+    if (window == RadarWindowKind::none) return std::is_integral_v<T>;
+    if (window == RadarWindowKind::explicit_fp32) return std::is_same_v<T, std::int32_t>;
+    return true;
+}
+
+// radartools_typed.cpp:280-286
+inline std::size_t radar_elements(int a, int b, const char* fn)
+{
+    const long long n = (long long)a * b;
+    if (a < 1 || b < 1 || n > std::numeric_limits<int>::max())
+        throw std::invalid_argument(std::string(fn) + " shape exceeds kernel capacity");
+    return (std::size_t)n;
+}
+
+// complex64 staging of TypedComplex<T> data (a plain view for T = float)
+template <class T>
+DeviceArray<ComplexFloat> staged_c64(const DeviceArray<TypedComplex<T>>& x)
+{
+    DeviceArray<ComplexFloat> out(x.size());
+    if (x.size())
+        zkx_check(zkx_convert_to_f32(x.data(), zkx_dtype<T>(), 2LL * (long long)x.size(),
+                                     reinterpret_cast<float*>(out.data()), nullptr));
+    return out;
+}
+
+inline void finish_complex(DeviceArray<ComplexFloat>&& computed, bool fp64, RadarComplexDeviceResult& r)
+{
+    r.is_fp64 = fp64;
+    if (fp64) {
+        r.fp64 = DeviceArray<ComplexDouble>(computed.size());
+        if (computed.size())
+            zkx_check(zkx_widen_f32_to_f64(reinterpret_cast<const float*>(computed.data()),
+                                           2LL * (long long)computed.size(),
+                                           reinterpret_cast<double*>(r.fp64.data()), nullptr));
+    } else {
+        r.fp32 = std::move(computed);
+    }
+}
+
+inline const float* window_pointer(RadarWindowKind kind, const DeviceArray<float>* w, std::size_t expected,
+                                   const char* fn)
+{
+    const int code = static_cast<int>(kind);
+    if (code < 0 || code > 4) throw std::invalid_argument(std::string("unsupported ") + fn + " window");
+    const bool needs = kind == RadarWindowKind::explicit_fp32 || kind == RadarWindowKind::explicit_fp64;
+    if (needs != (w != nullptr) || (w && w->size() != expected))
+        throw std::invalid_argument(std::string(fn) + " window is invalid");
+    return w ? w->data() : nullptr;
+}
+
+}  // namespace detail
+
+/// Matched filter of every pulse with the windowed, optionally normalised template.
+template <class T>
+RadarComplexDeviceResult pulse_compression_device(const DeviceArray<TypedComplex<T>>& x,
+                                                  const DeviceArray<TypedComplex<T>>& pulse_template,
+                                                  const PulseCompressionOptions& options,
+                                                  const DeviceArray<float>* explicit_window = nullptr)
+{
+    const int nfft = options.nfft == -1 ? options.samples_per_pulse : options.nfft;
+    const std::size_t in = detail::radar_elements(options.num_pulses, options.samples_per_pulse, "pulse_compression");
+    const std::size_t outc = detail::radar_elements(options.num_pulses, nfft, "pulse_compression");
+    if (nfft < 1 || x.size() != in || pulse_template.empty())
+        throw std::invalid_argument("pulse_compression shape is invalid");
+    const float* w = detail::window_pointer(options.window, explicit_window, pulse_template.size(), "pulse_compression");
+    DeviceArray<ComplexFloat> computed(outc);
+    if constexpr (std::is_same_v<T, float>) {
+        detail::zkx_check(zkx_pulse_compression_c64(x.data(), options.num_pulses, options.samples_per_pulse,
+                                                    pulse_template.data(), (int)pulse_template.size(), nfft,
+                                                    options.normalize ? 1 : 0, (int)options.window, w,
+                                                    computed.data(), nullptr));
+    } else {
+        auto xc = detail::staged_c64(x);
+        auto tc = detail::staged_c64(pulse_template);
+        detail::zkx_check(zkx_pulse_compression_c64(xc.data(), options.num_pulses, options.samples_per_pulse,
+                                                    tc.data(), (int)tc.size(), nfft, options.normalize ? 1 : 0,
+                                                    (int)options.window, w, computed.data(), nullptr));
+    }
+    RadarComplexDeviceResult r;
+    r.shape = {options.num_pulses, nfft};
+    detail::finish_complex(std::move(computed), detail::radar_result_is_fp64<T>(options.window), r);
+    return r;
+}
+
+/// FFT along pulses of window * x into a caller-allocated FP32 [nfft, samples] output.
+template <class T>
+void pulse_doppler_device(const DeviceArray<TypedComplex<T>>& x, const PulseDopplerOptions& options,
+                          DeviceArray<ComplexFloat>& output, const DeviceArray<float>* explicit_window = nullptr)
+{
+    const int nfft = options.nfft == -1 ? options.num_pulses : options.nfft;
+    const std::size_t in = detail::radar_elements(options.num_pulses, options.samples_per_pulse, "pulse_doppler");
+    const std::size_t outc = detail::radar_elements(nfft, options.samples_per_pulse, "pulse_doppler");
+    if (nfft < 1 || x.size() != in) throw std::invalid_argument("pulse_doppler shape is invalid");
+    const float* w = detail::window_pointer(options.window, explicit_window, (std::size_t)options.num_pulses,
+                                            "pulse_doppler");
+    if (output.size() != outc) throw std::invalid_argument("pulse_doppler preallocated output shape mismatch");
+    if constexpr (std::is_same_v<T, float>) {
+        detail::zkx_check(zkx_pulse_doppler_c64(x.data(), options.num_pulses, options.samples_per_pulse, nfft,
+                                                (int)options.window, w, output.data(), nullptr, nullptr));
+    } else {
+        auto xc = detail::staged_c64(x);
+        detail::zkx_check(zkx_pulse_doppler_c64(xc.data(), options.num_pulses, options.samples_per_pulse, nfft,
+                                                (int)options.window, w, output.data(), nullptr, nullptr));
+    }
+}
+
+template <class T>
+RadarComplexDeviceResult pulse_doppler_device(const DeviceArray<TypedComplex<T>>& x,
+                                              const PulseDopplerOptions& options,
+                                              const DeviceArray<float>* explicit_window = nullptr)
+{
+    const int nfft = options.nfft == -1 ? options.num_pulses : options.nfft;
+    DeviceArray<ComplexFloat> computed(detail::radar_elements(nfft, options.samples_per_pulse, "pulse_doppler"));
+    pulse_doppler_device(x, options, computed, explicit_window);
+    RadarComplexDeviceResult r;
+    r.shape = {nfft, options.samples_per_pulse};
+    detail::finish_complex(std::move(computed), detail::radar_result_is_fp64<T>(options.window), r);
+    return r;
+}
+
+/// alpha = reference * (pfa^(-1/reference) - 1), stored as one FP64 device value.
+template <class T>
+DeviceArray<double> cfar_alpha_device(T pfa, int reference)
+{
+    double p;
+    if constexpr (std::is_same_v<T, __half>) p = (double)__half2float(pfa);
+    else p = (double)pfa;
+    double alpha = 0.0;
+    detail::zkx_check(zkx_cfar_alpha(p, reference, &alpha));
+    return DeviceArray<double>::from_host(std::vector<double>{alpha});
+}
+
+/// CA-CFAR into caller-allocated threshold and detections (same element count as x).
+template <class T>
+void ca_cfar_device(const DeviceArray<T>& x, const std::vector<int>& shape, const CaCfarOptions& options,
+                    DeviceArray<float>& threshold, DeviceArray<CfarDetection>& detections)
+{
+    if (shape.size() > 2) throw std::invalid_argument("ca_cfar supports only scalar, 1D, or 2D input");
+    if (threshold.size() != x.size() || detections.size() != x.size())
+        throw std::invalid_argument("ca_cfar preallocated output shape must match input");
+    if (shape.empty()) {
+        if (x.size() != 1) throw std::invalid_argument("ca_cfar scalar input must contain one element");
+        // rank 0: threshold 0 and the plain comparison (radartools_typed.cpp:170-173, 550-553)
+        auto xf = detail::staged_f32<T>(x.data(), 1);
+        const float v = xf.to_host()[0];
+        const float zero = 0.0f;
+        cuda_utils::copy_to_device(threshold.data(), &zero, 1);
+        const CfarDetection d = v > 0.0f ? CfarDetection::yes : CfarDetection::no;
+        cuda_utils::copy_to_device(detections.data(), &d, 1);
+        cuda_utils::synchronize_stream();
+        return;
+    }
+    if (options.guard_cells.size() != shape.size() || options.reference_cells.size() != shape.size())
+        throw std::invalid_argument("ca_cfar cell parameter rank mismatch");
+    const int rank = (int)shape.size();
+    const int rows = shape[0], cols = rank == 2 ? shape[1] : 1;
+    if ((long long)rows * cols != (long long)x.size()) throw std::invalid_argument("ca_cfar input size or capacity is invalid");
+    auto xf = detail::staged_f32<T>(x.data(), x.size());
+    const int g1 = rank == 2 ? options.guard_cells[1] : 0;
+    const int r1 = rank == 2 ? options.reference_cells[1] : 0;
+    auto* det = reinterpret_cast<uint8_t*>(detections.data());
+    detail::zkx_check(zkx_ca_cfar_f32(xf.data(), rank, rows, cols, options.guard_cells[0], g1,
+                                      options.reference_cells[0], r1, options.pfa, ZKX_CFAR_COMPAT,
+                                      threshold.data(), det, nullptr));
+    if constexpr (std::is_integral_v<T>)
+        detail::zkx_check(zkx_cfar_detect_int(x.data(), detail::zkx_dtype<T>(), threshold.data(),
+                                              (long long)x.size(), det, nullptr));
+}
+
+template <class T>
+CaCfarDeviceResult ca_cfar_device(const DeviceArray<T>& x, const std::vector<int>& shape,
+                                  const CaCfarOptions& options)
+{
+    CaCfarDeviceResult r;
+    r.shape = shape;
+    r.threshold = DeviceArray<float>(x.size());
+    r.detections = DeviceArray<CfarDetection>(x.size());
+    ca_cfar_device(x, shape, options, r.threshold, r.detections);
+    return r;
+}
+
+// CPU references (declared for callers that link the reference's own CPU implementation).
+template <class T>
+CaCfarCpuResult ca_cfar_typed_cpu(const std::vector<T>& x, const std::vector<int>& shape, const CaCfarOptions& options);
+template <class T>
+double cfar_alpha_typed_cpu(T pfa, int reference);
+template <class T>
+RadarComplexCpuResult pulse_compression_typed_cpu(const std::vector<TypedComplex<T>>& x,
+                                                  const std::vector<TypedComplex<T>>& pulse_template,
+                                                  const PulseCompressionOptions& options,
+                                                  const std::vector<float>* explicit_window = nullptr);
+template <class T>
+RadarComplexCpuResult pulse_doppler_typed_cpu(const std::vector<TypedComplex<T>>& x,
+                                              const PulseDopplerOptions& options,
+                                              const std::vector<float>* explicit_window = nullptr);
+
+}  // namespace cusignal

@@ -56,6 +56,15 @@ enum {
     ZKX_WINDOW_EXPLICIT_FP64 = 4
 };
 
+/* Business dtypes of the reference's operators (TypedComplex<T> components). */
+enum {
+    ZKX_DTYPE_F32 = 0,
+    ZKX_DTYPE_F16 = 1,
+    ZKX_DTYPE_I32 = 2,
+    ZKX_DTYPE_I16 = 3,
+    ZKX_DTYPE_I8 = 4
+};
+
 /* CA-CFAR evaluation modes. */
 enum {
     /* Separable training-ring sums in FP32 with every cell whose power lies within
@@ -130,6 +139,13 @@ ZKX_API int zkx_pulse_doppler_c64(const void* x, int num_pulses, int samples_per
                           int window_kind, const float* explicit_window, void* out,
                           float* power, zkx_stream_t stream);
 
+/* Batched complex-to-complex FFT of `batch` contiguous rows of n complex64 (n a power of
+ * two, 1..16384); forward unnormalised, inverse scaled by 1/n; x == y allowed.
+ * Replaces FFTInterface::fft_batch_device / ifft_batch_device
+ * (include/cusignal/backends/fft/fft_interface.h:499-536; fft_interface.cpp:385-470). */
+ZKX_API int zkx_fft_c2c_c64(const void* x, int batch, int n, int inverse, void* y,
+                            zkx_stream_t stream);
+
 /* CFAR threshold multiplier alpha = N_ref * (pfa^(-1/N_ref) - 1), on the host in FP64.
  * Replaces cusignal::cfar_alpha_typed_cpu / cfar_alpha_device (radartools_typed.h:207-222,
  * radartools_typed.cpp:592-617). */
@@ -188,6 +204,11 @@ ZKX_API int zkx_resample_poly_layout(int n, int up, int down, int custom_coeffic
 ZKX_API int zkx_resample_poly_design(const zkx_resample_layout* layout, double kaiser_beta,
                              double* taps);
 
+/* The same windowed-sinc design with a caller-supplied window of coefficient_count values
+ * (the reference's Hamming and explicit design windows, filtering_typed.cpp:195-204). */
+ZKX_API int zkx_resample_poly_design_window(const zkx_resample_layout* layout, const double* window,
+                                            double* taps);
+
 /* Centred polyphase resampling along the last axis of [lines, n] with FP32 device
  * taps (already scaled by up).  Replaces the compute half of
  * cusignal::resample_poly_device<float> (filtering_typed.h:765-770;
@@ -195,6 +216,28 @@ ZKX_API int zkx_resample_poly_design(const zkx_resample_layout* layout, double k
  * [lines, layout->output_samples]. */
 ZKX_API int zkx_resample_poly_f32(const float* x, int lines, int n, const zkx_resample_layout* layout,
                           const float* taps, float* y, zkx_stream_t stream);
+
+/* dst[i] = (float)src[i] for `count` scalars of `dtype` (complex data: 2 scalars per
+ * element).  Replaces the reference's dtype staging before FP32 compute
+ * (src/operators/filtering/filtering_kernels.cuh:1277 convert_signal_kernel,
+ * radartools_kernels.cuh:215-237 pack kernels). */
+ZKX_API int zkx_convert_to_f32(const void* src, int dtype, long long count, float* dst,
+                               zkx_stream_t stream);
+
+/* Integral CA-CFAR decision of the reference (radartools_kernels.cuh:24-37) for int32/16/8
+ * input x and FP32 thresholds: detections[i] = x[i] > floor(threshold[i]) with NaN and
+ * range saturation rules. */
+ZKX_API int zkx_cfar_detect_int(const void* x, int dtype, const float* threshold, long long count,
+                                uint8_t* detections, zkx_stream_t stream);
+
+/* dst[c, r] = src[r, c] for a row-major [rows, cols] FP32 array (moves a filtering axis
+ * last; no counterpart in the reference, whose kernels take axis strides). */
+ZKX_API int zkx_transpose_f32(const float* src, int rows, int cols, float* dst, zkx_stream_t stream);
+
+/* dst[i] = (double)src[i]: exact widening of FP32 results to the reference's FP64 result
+ * storage (src/runtime/fp64_storage_finalize.cu:45-87). */
+ZKX_API int zkx_widen_f32_to_f64(const float* src, long long count, double* dst,
+                                 zkx_stream_t stream);
 
 /* ------------------------------------------------------------ the fused chain */
 

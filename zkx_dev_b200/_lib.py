@@ -48,6 +48,7 @@ SIGNATURES = {
     "zkx_replica_spectrum_c64": (_I, [_P, _I, _I, _I, _I, _P, _P, _P]),
     "zkx_pulse_compression_spectrum_c64": (_I, [_P, _I, _I, _I, _P, _P, _P]),
     "zkx_pulse_doppler_c64": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, _P]),
+    "zkx_fft_c2c_c64": (_I, [_P, _I, _I, _I, _P, _P]),
     "zkx_cfar_alpha": (_I, [_D, _I, ctypes.POINTER(_D)]),
     "zkx_cfar_reference_count": (_I, [_I, _I, _I, _I, _I]),
     "zkx_ca_cfar_f32": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _D, _I, _P, _P, _P]),
@@ -57,6 +58,11 @@ SIGNATURES = {
     "zkx_resample_poly_layout": (_I, [_I, _I, _I, _I, _I, ctypes.POINTER(ResampleLayout)]),
     "zkx_resample_poly_design": (_I, [ctypes.POINTER(ResampleLayout), _D, _P]),
     "zkx_resample_poly_f32": (_I, [_P, _I, _I, ctypes.POINTER(ResampleLayout), _P, _P, _P]),
+    "zkx_convert_to_f32": (_I, [_P, _I, ctypes.c_longlong, _P, _P]),
+    "zkx_widen_f32_to_f64": (_I, [_P, ctypes.c_longlong, _P, _P]),
+    "zkx_cfar_detect_int": (_I, [_P, _I, _P, ctypes.c_longlong, _P, _P]),
+    "zkx_transpose_f32": (_I, [_P, _I, _I, _P, _P]),
+    "zkx_resample_poly_design_window": (_I, [ctypes.POINTER(ResampleLayout), _P, _P]),
     "zkx_rd_plan_create": (_I, [ctypes.POINTER(RdDesc), _P, _P, _P, _P, ctypes.POINTER(_P)]),
     "zkx_rd_plan_destroy": (_I, [_P]),
     "zkx_rd_plan_shape": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),

@@ -144,6 +144,17 @@ extern "C" int zkx_pulse_doppler_c64(const void* x, int P, int N, int nfft, int 
                                 static_cast<float2*>(out), power, stream);
 }
 
+extern "C" int zkx_fft_c2c_c64(const void* x, int batch, int n, int inverse, void* y,
+                               zkx_stream_t stream)
+{
+    ZKX_TRY(check_radar_shape(batch, n, "fft"));
+    if (!x || !y) return fail(ZKX_INVALID_ARGUMENT, "fft: null pointer");
+    ZKX_TRY(check_transform_length(n, "fft"));
+    ZKX_TRY(ensure_device_ready());
+    return launch_fft_rows(static_cast<const float2*>(x), batch, n, inverse ? 1 : 0,
+                           static_cast<float2*>(y), stream);
+}
+
 // ------------------------------------------------------------------------ CFAR
 
 extern "C" int zkx_cfar_alpha(double pfa, int reference_count, double* alpha)
@@ -292,6 +303,26 @@ extern "C" int zkx_resample_poly_design(const zkx_resample_layout* L, double bet
         const int off = i - half;
         const double sinc = off == 0 ? cutoff : std::sin(pi * cutoff * off) / (pi * off);
         taps[i] = sinc * w;
+        scale += taps[i];
+    }
+    for (int i = 0; i < count; ++i) taps[i] = taps[i] / scale * L->up;
+    return ZKX_SUCCESS;
+}
+
+extern "C" int zkx_resample_poly_design_window(const zkx_resample_layout* L, const double* window,
+                                               double* taps)
+{
+    // filtering_typed.cpp:208-222 with the window supplied by the caller
+    if (!L || !window || !taps) return fail(ZKX_INVALID_ARGUMENT, "resample_poly_design_window: null pointer");
+    const int count = L->coefficient_count, half = L->half_length;
+    if (count < 1) return fail(ZKX_INVALID_ARGUMENT, "resample_poly_design_window: empty design");
+    const double cutoff = 1.0 / (L->up > L->down ? L->up : L->down);
+    const double pi = 3.1415926535897932384626433832795;
+    double scale = 0.0;
+    for (int i = 0; i < count; ++i) {
+        const int off = i - half;
+        const double sinc = off == 0 ? cutoff : std::sin(pi * cutoff * off) / (pi * off);
+        taps[i] = sinc * window[i];
         scale += taps[i];
     }
     for (int i = 0; i < count; ++i) taps[i] = taps[i] / scale * L->up;

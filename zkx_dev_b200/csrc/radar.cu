@@ -199,6 +199,41 @@ pulse_compression_persistent_kernel(const float2* __restrict__ x, int pulses, in
     }
 }
 
+// Batched C2C transform of contiguous rows: forward unnormalised, inverse scaled by 1/N
+// (the convention of the reference's FFTInterface, fft_interface.h:39-42).  Each row is
+// held in registers before any store, so in-place calls (x == y) are safe.
+template <int N, int G, int DIR>
+__global__ void __launch_bounds__(G * FftPlan<N, elems_for(N)>::T)
+fft_rows_kernel(const float2* x, int rows, float2* y, const float2* __restrict__ tw)
+{
+    using PL = FftPlan<N, elems_for(N)>;
+    extern __shared__ float2 sm[];
+    const int g = threadIdx.x / PL::T;
+    const int t = threadIdx.x - g * PL::T;
+    const int row = blockIdx.x * G + g;
+    const bool active = row < rows;
+    constexpr int S = PL::smem_elems() % 16 == 0 && PL::T < 16 ? PL::smem_elems() + 8 : PL::smem_elems();
+    float2* smg = sm + g * S;
+    const float2* xr = x + (size_t)row * N;
+    float2 v[PL::E];
+#pragma unroll
+    for (int r = 0; r < PL::E; ++r) v[r] = active ? xr[t + PL::T * r] : make_float2(0.f, 0.f);
+    fft_block<PL, DIR, 1>(v, smg, t, tw);
+    if (active) {
+        float2* yr = y + (size_t)row * N;
+        constexpr float scale = DIR > 0 ? 1.0f / (float)N : 1.0f;
+#pragma unroll
+        for (int r = 0; r < PL::E; ++r) {
+            float2 o = v[r];
+            if (DIR > 0) {
+                o.x *= scale;
+                o.y *= scale;
+            }
+            yr[t + PL::T * r] = o;
+        }
+    }
+}
+
 // ------------------------------------------------------------------- Doppler
 
 // Range columns per Doppler CTA: 16 (128-byte row segments per warp load, a
@@ -407,6 +442,28 @@ int doppler_impl(const float2* x, int pulses, int samples, const float* window, 
     return ZKX_SUCCESS;
 }
 
+template <int N>
+int fft_rows_impl(const float2* x, int rows, int inverse, float2* y, cudaStream_t s)
+{
+    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
+    using PL = FftPlan<N, elems_for(N)>;
+    constexpr int G = rows_per_cta(N);
+    constexpr int S = PL::smem_elems() % 16 == 0 && PL::T < 16 ? PL::smem_elems() + 8 : PL::smem_elems();
+    const size_t smem = (size_t)G * S * sizeof(float2);
+    const int blocks = (rows + G - 1) / G;
+    if (inverse) {
+        auto k = fft_rows_kernel<N, G, 1>;
+        ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k<<<blocks, G * PL::T, smem, s>>>(x, rows, y, twiddle_table());
+    } else {
+        auto k = fft_rows_kernel<N, G, -1>;
+        ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k<<<blocks, G * PL::T, smem, s>>>(x, rows, y, twiddle_table());
+    }
+    ZKX_LAUNCHED("fft_rows_kernel");
+    return ZKX_SUCCESS;
+}
+
 #define ZKX_DISPATCH_POW2(LOG, CALL)                                                    \
     switch (LOG) {                                                                      \
     case 0: return CALL(1);     case 1: return CALL(2);     case 2: return CALL(4);     \
@@ -442,6 +499,13 @@ int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft, con
     if (nfft > 4096) return fail(ZKX_UNSUPPORTED_OPERATION, "pulse_doppler: nfft above 4096 is not supported");
 #define ZKX_CALL(NN) doppler_impl<NN>(x, pulses, samples, window, out, power, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
+#undef ZKX_CALL
+}
+
+int launch_fft_rows(const float2* x, int rows, int n, int inverse, float2* y, cudaStream_t stream)
+{
+#define ZKX_CALL(NN) fft_rows_impl<NN>(x, rows, inverse, y, stream)
+    ZKX_DISPATCH_POW2(ilog2_host(n), ZKX_CALL)
 #undef ZKX_CALL
 }
 

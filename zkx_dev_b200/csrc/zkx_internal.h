@@ -60,6 +60,7 @@ int launch_pulse_compression(const float2* x, int pulses, int samples, int nfft,
                              const float2* spectrum, float2* y, cudaStream_t stream);
 int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft,
                          const float* window, float2* out, float* power, cudaStream_t stream);
+int launch_fft_rows(const float2* x, int rows, int n, int inverse, float2* y, cudaStream_t stream);
 int launch_doppler_window(int pulses, int window_kind, const float* explicit_window, float* out,
                           cudaStream_t stream);
 int launch_ca_cfar_accurate(const float* x, int rows, int columns, int guard_rows,
