@@ -269,10 +269,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict:
     clk = clocks.stop()
 
     if dist is not None:
-        import torch.distributed as tdist
-        t = torch.tensor([elapsed_ms, e2e_ms], device=dev)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        elapsed_ms, e2e_ms = float(t[0]), float(t[1])
+        from zkx_dev_b200.replicas import max_over_ranks
+        elapsed_ms, e2e_ms = max_over_ranks([elapsed_ms, e2e_ms], dist, dev)
 
     chain.close()
     per_stage = {k: statistics.median(v) for k, v in stage_ms.items()}
