@@ -280,6 +280,23 @@ ZKX_API int zkx_rd_plan_shape(zkx_rd_plan plan, int* range_bins, int* doppler_bi
 ZKX_API int zkx_rd_execute(zkx_rd_plan plan, const void* x, void* compressed, void* rd, float* power,
                    float* threshold, uint8_t* detections, zkx_stream_t stream);
 
+/* The chain on `batch` CPIs stored back to back (x [batch, P, N]; outputs [batch, ...]),
+ * one launch per stage for the whole batch (no counterpart in the reference, which runs
+ * one CPI per call). */
+ZKX_API int zkx_rd_execute_batch(zkx_rd_plan plan, const void* x, int batch, void* compressed,
+                                 void* rd, float* power, float* threshold, uint8_t* detections,
+                                 zkx_stream_t stream);
+
+/* A CUDA graph of one zkx_rd_execute_batch with fixed pointers: create runs the chain once
+ * eagerly (allocating any plan-owned buffer), then captures and instantiates it; launch
+ * replays it on `stream` with one call.  No counterpart in the reference. */
+typedef struct zkx_rd_graph_s* zkx_rd_graph;
+ZKX_API int zkx_rd_graph_create(zkx_rd_plan plan, const void* x, int batch, void* compressed,
+                                void* rd, float* power, float* threshold, uint8_t* detections,
+                                zkx_rd_graph* graph);
+ZKX_API int zkx_rd_graph_launch(zkx_rd_graph graph, zkx_stream_t stream);
+ZKX_API int zkx_rd_graph_destroy(zkx_rd_graph graph);
+
 #ifdef __cplusplus
 }
 #endif

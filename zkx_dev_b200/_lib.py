@@ -67,6 +67,10 @@ SIGNATURES = {
     "zkx_rd_plan_destroy": (_I, [_P]),
     "zkx_rd_plan_shape": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "zkx_rd_execute": (_I, [_P, _P, _P, _P, _P, _P, _P, _P]),
+    "zkx_rd_execute_batch": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, _P]),
+    "zkx_rd_graph_create": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, ctypes.POINTER(_P)]),
+    "zkx_rd_graph_launch": (_I, [_P, _P]),
+    "zkx_rd_graph_destroy": (_I, [_P]),
 }
 
 _lib: Optional[ctypes.CDLL] = None

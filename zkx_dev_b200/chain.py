@@ -67,15 +67,17 @@ class RangeDopplerChain:
         self.range_bins, self.doppler_bins = nr.value, nd.value
         self.device = dev
 
-    def allocate_outputs(self, keep_compressed: bool = True, keep_rd: bool = True) -> Dict[str, Optional[torch.Tensor]]:
+    def allocate_outputs(self, keep_compressed: bool = True, keep_rd: bool = True,
+                         batch: Optional[int] = None) -> Dict[str, Optional[torch.Tensor]]:
         P, nr, nd = self.cfg.num_pulses, self.range_bins, self.doppler_bins
         dev = self.device
+        lead = () if batch is None else (batch,)
         return {
-            "compressed": torch.empty((P, nr), dtype=torch.complex64, device=dev) if keep_compressed else None,
-            "rd": torch.empty((nd, nr), dtype=torch.complex64, device=dev) if keep_rd else None,
-            "power": torch.empty((nd, nr), dtype=torch.float32, device=dev),
-            "threshold": torch.empty((nd, nr), dtype=torch.float32, device=dev),
-            "detections": torch.empty((nd, nr), dtype=torch.uint8, device=dev),
+            "compressed": torch.empty(lead + (P, nr), dtype=torch.complex64, device=dev) if keep_compressed else None,
+            "rd": torch.empty(lead + (nd, nr), dtype=torch.complex64, device=dev) if keep_rd else None,
+            "power": torch.empty(lead + (nd, nr), dtype=torch.float32, device=dev),
+            "threshold": torch.empty(lead + (nd, nr), dtype=torch.float32, device=dev),
+            "detections": torch.empty(lead + (nd, nr), dtype=torch.uint8, device=dev),
         }
 
     def run(self, x: torch.Tensor, out: Optional[Dict[str, Optional[torch.Tensor]]] = None):
@@ -92,10 +94,59 @@ class RangeDopplerChain:
 
     __call__ = run
 
+    def run_batch(self, x: torch.Tensor, out: Optional[Dict[str, Optional[torch.Tensor]]] = None):
+        """The chain on a stack of CPIs x [B, P, N] with one launch per stage."""
+        if not isinstance(x, torch.Tensor) or not x.is_cuda or x.dtype != torch.complex64 or x.ndim != 3:
+            raise TypeError("x must be a complex64 CUDA tensor [B, P, N]")
+        x = x.contiguous()
+        if tuple(x.shape[1:]) != (self.cfg.num_pulses, self.cfg.samples_per_pulse):
+            raise ValueError("CPI shape does not match the plan")
+        B = x.shape[0]
+        if out is None:
+            out = self.allocate_outputs(batch=B)
+        L.check(L.lib().zkx_rd_execute_batch(self._plan, x.data_ptr(), B, L.ptr(out["compressed"]),
+                                             L.ptr(out["rd"]), L.ptr(out["power"]),
+                                             out["threshold"].data_ptr(), out["detections"].data_ptr(),
+                                             L.stream_handle()))
+        return out
+
+    def capture(self, x: torch.Tensor, out: Dict[str, Optional[torch.Tensor]]) -> "ChainGraph":
+        """A CUDA graph replaying run_batch(x, out) (fixed tensors) with one launch."""
+        x = x.contiguous()
+        B = x.shape[0] if x.ndim == 3 else 1
+        g = ctypes.c_void_p()
+        L.check(L.lib().zkx_rd_graph_create(self._plan, x.data_ptr(), B, L.ptr(out["compressed"]),
+                                            L.ptr(out["rd"]), L.ptr(out["power"]),
+                                            out["threshold"].data_ptr(), out["detections"].data_ptr(),
+                                            ctypes.byref(g)))
+        return ChainGraph(g, (x, out, self))
+
     def close(self) -> None:
         if getattr(self, "_plan", None) is not None and self._plan.value:
             L.lib().zkx_rd_plan_destroy(self._plan)
             self._plan = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ChainGraph:
+    """An instantiated CUDA graph of the chain; replay with launch()."""
+
+    def __init__(self, handle: ctypes.c_void_p, keep):
+        self._g = handle
+        self._keep = keep
+
+    def launch(self) -> None:
+        L.check(L.lib().zkx_rd_graph_launch(self._g, L.stream_handle()))
+
+    def close(self) -> None:
+        if self._g is not None and self._g.value:
+            L.lib().zkx_rd_graph_destroy(self._g)
+            self._g = ctypes.c_void_p()
 
     def __del__(self):
         try:

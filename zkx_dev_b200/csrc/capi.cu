@@ -141,7 +141,7 @@ extern "C" int zkx_pulse_doppler_c64(const void* x, int P, int N, int nfft, int 
         ZKX_TRY(launch_doppler_window(P, kind, w, win, stream));
     }
     return launch_pulse_doppler(static_cast<const float2*>(x), P, N, nfft, win,
-                                static_cast<float2*>(out), power, stream);
+                                static_cast<float2*>(out), power, 1, stream);
 }
 
 extern "C" int zkx_fft_c2c_c64(const void* x, int batch, int n, int inverse, void* y,
@@ -192,7 +192,7 @@ extern "C" int zkx_ca_cfar_f32(const float* x, int rank, int rows, int cols, int
                                      detections, stream);
     }
     return launch_ca_cfar_accurate(x, rows, cols, gr, gc, rr, rc, g.alpha, g.nref, threshold,
-                                   detections, stream);
+                                   detections, 1, stream);
 }
 
 // --------------------------------------------------------------------- filters
@@ -358,8 +358,11 @@ struct zkx_rd_plan_s {
     float2* spectrum = nullptr;
     float* doppler_window = nullptr;
     float2* compressed = nullptr;  // used when the caller passes no compressed buffer
+    size_t compressed_elems = 0;
     float* power = nullptr;        // used when the caller passes no power buffer
+    size_t power_elems = 0;
     float* cumulative = nullptr;   // compat CFAR integral image
+    size_t cumulative_elems = 0;
     CfarGeometry cfar;
 };
 
@@ -406,8 +409,10 @@ extern "C" int zkx_rd_plan_create(const zkx_rd_desc* d, const void* replica,
     cudaError_t e = cudaMalloc(&p->spectrum, (size_t)nr * sizeof(float2));
     if (e == cudaSuccess && d->doppler_window != ZKX_WINDOW_NONE)
         e = cudaMalloc(&p->doppler_window, (size_t)P * sizeof(float));
-    if (e == cudaSuccess && d->cfar_mode == ZKX_CFAR_COMPAT)
+    if (e == cudaSuccess && d->cfar_mode == ZKX_CFAR_COMPAT) {
         e = cudaMalloc(&p->cumulative, (size_t)nd * nr * sizeof(float));
+        if (e == cudaSuccess) p->cumulative_elems = (size_t)nd * nr;
+    }
     if (e != cudaSuccess) {
         release_plan(p);
         return cuda_status(e, "rd_plan_create allocation");
@@ -439,31 +444,126 @@ extern "C" int zkx_rd_plan_shape(zkx_rd_plan plan, int* range_bins, int* doppler
     return ZKX_SUCCESS;
 }
 
+extern "C" int zkx_rd_execute_batch(zkx_rd_plan p, const void* x, int batch, void* compressed,
+                                    void* rd, float* power, float* threshold, uint8_t* detections,
+                                    zkx_stream_t stream)
+{
+    if (!p || !x || !threshold || !detections) return fail(ZKX_INVALID_ARGUMENT, "rd_execute: null pointer");
+    if (batch < 1) return fail(ZKX_INVALID_SHAPE, "rd_execute: batch must be positive");
+    const int P = p->d.num_pulses, N = p->d.samples_per_pulse;
+    const int nr = p->range_nfft, nd = p->doppler_nfft;
+    if ((long long)batch * P * (nr > N ? nr : N) > INT_MAX || (long long)batch * nd * nr > INT_MAX)
+        return fail(ZKX_INVALID_SHAPE, "rd_execute: batch exceeds kernel capacity");
+    const size_t cube = (size_t)batch * P * nr, map = (size_t)batch * nd * nr;
+    if (!compressed) {
+        if (p->compressed_elems < cube) {
+            cudaFree(p->compressed);
+            p->compressed = nullptr;
+            p->compressed_elems = 0;
+            ZKX_CUDA(cudaMalloc(&p->compressed, cube * sizeof(float2)));
+            p->compressed_elems = cube;
+        }
+        compressed = p->compressed;
+    }
+    if (!power) {
+        if (p->power_elems < map) {
+            cudaFree(p->power);
+            p->power = nullptr;
+            p->power_elems = 0;
+            ZKX_CUDA(cudaMalloc(&p->power, map * sizeof(float)));
+            p->power_elems = map;
+        }
+        power = p->power;
+    }
+    if (p->d.cfar_mode == ZKX_CFAR_COMPAT && p->cumulative_elems < (size_t)nd * nr)
+        return fail(ZKX_INTERNAL_ERROR, "rd_execute: compat workspace missing");
+    // the CPIs of a batch are contiguous, so range compression sees batch*P pulses
+    ZKX_TRY(launch_pulse_compression(static_cast<const float2*>(x), batch * P, N, nr, p->spectrum,
+                                     static_cast<float2*>(compressed), stream));
+    ZKX_TRY(launch_pulse_doppler(static_cast<const float2*>(compressed), P, nr, nd,
+                                 p->doppler_window, static_cast<float2*>(rd), power, batch, stream));
+    const int* gd = p->d.guard_cells;
+    const int* rf = p->d.reference_cells;
+    if (p->d.cfar_mode == ZKX_CFAR_COMPAT) {
+        for (int b = 0; b < batch; ++b)
+            ZKX_TRY(launch_ca_cfar_compat(power + (size_t)b * nd * nr, 2, nd, nr, gd[0], gd[1], rf[0], rf[1],
+                                          (float)p->cfar.alpha, p->cfar.nref, p->cumulative,
+                                          threshold + (size_t)b * nd * nr, detections + (size_t)b * nd * nr,
+                                          stream));
+        return ZKX_SUCCESS;
+    }
+    return launch_ca_cfar_accurate(power, nd, nr, gd[0], gd[1], rf[0], rf[1], p->cfar.alpha,
+                                   p->cfar.nref, threshold, detections, batch, stream);
+}
+
 extern "C" int zkx_rd_execute(zkx_rd_plan p, const void* x, void* compressed, void* rd,
                               float* power, float* threshold, uint8_t* detections,
                               zkx_stream_t stream)
 {
-    if (!p || !x || !threshold || !detections) return fail(ZKX_INVALID_ARGUMENT, "rd_execute: null pointer");
-    const int P = p->d.num_pulses, N = p->d.samples_per_pulse;
-    const int nr = p->range_nfft, nd = p->doppler_nfft;
-    if (!compressed) {
-        if (!p->compressed) ZKX_CUDA(cudaMalloc(&p->compressed, (size_t)P * nr * sizeof(float2)));
-        compressed = p->compressed;
+    return zkx_rd_execute_batch(p, x, 1, compressed, rd, power, threshold, detections, stream);
+}
+
+// ------------------------------------------------------------ graph capture
+
+struct zkx_rd_graph_s {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" int zkx_rd_graph_create(zkx_rd_plan p, const void* x, int batch, void* compressed, void* rd,
+                                   float* power, float* threshold, uint8_t* detections,
+                                   zkx_rd_graph* out)
+{
+    if (!out) return fail(ZKX_INVALID_ARGUMENT, "rd_graph_create: null pointer");
+    *out = nullptr;
+    // one eager run first: allocates plan-owned buffers and sets kernel attributes, so
+    // the captured launches neither allocate nor change state
+    cudaStream_t s;
+    ZKX_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    int rc = zkx_rd_execute_batch(p, x, batch, compressed, rd, power, threshold, detections, s);
+    if (rc == ZKX_SUCCESS) {
+        const cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = cuda_status(e, "rd_graph_create warm-up");
     }
-    if (!power) {
-        if (!p->power) ZKX_CUDA(cudaMalloc(&p->power, (size_t)nd * nr * sizeof(float)));
-        power = p->power;
+    cudaGraph_t graph = nullptr;
+    if (rc == ZKX_SUCCESS) {
+        cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) rc = cuda_status(e, "cudaStreamBeginCapture");
+        else {
+            rc = zkx_rd_execute_batch(p, x, batch, compressed, rd, power, threshold, detections, s);
+            e = cudaStreamEndCapture(s, &graph);
+            if (rc == ZKX_SUCCESS && e != cudaSuccess) rc = cuda_status(e, "cudaStreamEndCapture");
+        }
     }
-    ZKX_TRY(launch_pulse_compression(static_cast<const float2*>(x), P, N, nr, p->spectrum,
-                                     static_cast<float2*>(compressed), stream));
-    ZKX_TRY(launch_pulse_doppler(static_cast<const float2*>(compressed), P, nr, nd,
-                                 p->doppler_window, static_cast<float2*>(rd), power, stream));
-    const int* gd = p->d.guard_cells;
-    const int* rf = p->d.reference_cells;
-    if (p->d.cfar_mode == ZKX_CFAR_COMPAT)
-        return launch_ca_cfar_compat(power, 2, nd, nr, gd[0], gd[1], rf[0], rf[1],
-                                     (float)p->cfar.alpha, p->cfar.nref, p->cumulative, threshold,
-                                     detections, stream);
-    return launch_ca_cfar_accurate(power, nd, nr, gd[0], gd[1], rf[0], rf[1], p->cfar.alpha,
-                                   p->cfar.nref, threshold, detections, stream);
+    cudaGraphExec_t exec = nullptr;
+    if (rc == ZKX_SUCCESS) {
+        const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e != cudaSuccess) rc = cuda_status(e, "cudaGraphInstantiate");
+    }
+    cudaStreamDestroy(s);
+    if (rc != ZKX_SUCCESS) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    auto* g = new zkx_rd_graph_s;
+    g->graph = graph;
+    g->exec = exec;
+    *out = g;
+    return ZKX_SUCCESS;
+}
+
+extern "C" int zkx_rd_graph_launch(zkx_rd_graph g, zkx_stream_t stream)
+{
+    if (!g) return fail(ZKX_INVALID_ARGUMENT, "rd_graph_launch: null graph");
+    ZKX_CUDA(cudaGraphLaunch(g->exec, stream));
+    return ZKX_SUCCESS;
+}
+
+extern "C" int zkx_rd_graph_destroy(zkx_rd_graph g)
+{
+    if (!g) return ZKX_SUCCESS;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return ZKX_SUCCESS;
 }

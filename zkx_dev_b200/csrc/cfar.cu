@@ -72,6 +72,9 @@ cfar_accurate_kernel(const float* __restrict__ x, int rows, int cols, float scal
     float* SB = SA + TY * PITCH;          // [TY][PITCH] guard-row column sums
     const int r0 = blockIdx.y * TY;
     const int c0 = blockIdx.x * TX;
+    x += (size_t)blockIdx.z * rows * cols;  // map of a stacked batch
+    thr += (size_t)blockIdx.z * rows * cols;
+    det += (size_t)blockIdx.z * rows * cols;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int WARPS = kCfarThreads / 32;
 
@@ -251,11 +254,16 @@ cfar_accurate_tma_kernel(const __grid_constant__ CUtensorMap tmap, int rows, int
     uint64_t* bar = reinterpret_cast<uint64_t*>(SB + TY * PITCH);
     const int r0 = blockIdx.y * TY;
     const int c0 = blockIdx.x * TX;
+    // map of a stacked batch: its rows follow the previous map's; halo rows that reach a
+    // neighbouring map only feed border cells, whose threshold is 0
+    const int map_row0 = blockIdx.z * rows;
+    thr += (size_t)blockIdx.z * rows * cols;
+    det += (size_t)blockIdx.z * rows * cols;
     if (threadIdx.x == 0) mbar_init(bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(bar, (uint32_t)(G::HR * BOXW * sizeof(float)));
-        tma_load_2d(P, &tmap, c0 - MC - OFF, r0 - MR, bar);
+        tma_load_2d(P, &tmap, c0 - MC - OFF, map_row0 + r0 - MR, bar);
     }
     const bool ok = mbar_wait_bounded(bar, 0);
     if (__syncthreads_or(!ok)) {
@@ -374,6 +382,9 @@ __global__ void cfar_generic_kernel(const float* __restrict__ x, int rows, int c
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (long long)rows * cols) return;
+    x += (size_t)blockIdx.y * rows * cols;
+    thr += (size_t)blockIdx.y * rows * cols;
+    det += (size_t)blockIdx.y * rows * cols;
     const int r = (int)(i / cols), c = (int)(i % cols);
     const int mr = gr + rr, mc = gc + rc;
     const float xv = x[i];
@@ -489,13 +500,13 @@ __global__ void compat_threshold_kernel(const float* __restrict__ x, const float
 
 template <int GR, int GC, int RR, int RC>
 int accurate_impl(const float* x, int rows, int cols, float s32, double s64, float* thr,
-                  uint8_t* det, cudaStream_t s)
+                  uint8_t* det, int batch, cudaStream_t s)
 {
-    dim3 grid((cols + kCfarTX - 1) / kCfarTX, (rows + kCfarTY - 1) / kCfarTY);
+    dim3 grid((cols + kCfarTX - 1) / kCfarTX, (rows + kCfarTY - 1) / kCfarTY, batch);
     using G = CfarTmaGeom<GR, GC, RR, RC>;
     if ((cols & 3) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
         CUtensorMap map;
-        if (encode_tensor_map_2d_f32(&map, x, (uint64_t)cols, (uint64_t)rows,
+        if (encode_tensor_map_2d_f32(&map, x, (uint64_t)cols, (uint64_t)rows * batch,
                                      (uint64_t)cols * sizeof(float), G::BOXW, G::HR)) {
             const size_t smem = G::smem_bytes();
             auto k = cfar_accurate_tma_kernel<GR, GC, RR, RC>;
@@ -519,19 +530,20 @@ int accurate_impl(const float* x, int rows, int cols, float s32, double s64, flo
 
 int launch_ca_cfar_accurate(const float* x, int rows, int columns, int gr, int gc, int rr, int rc,
                             double alpha, int nref, float* threshold, uint8_t* detections,
-                            cudaStream_t stream)
+                            int batch, cudaStream_t stream)
 {
+    if (batch < 1 || batch > 65535) return fail(ZKX_UNSUPPORTED_OPERATION, "ca_cfar: batch must be 1..65535");
     const double s64 = alpha / (double)nref;
     const float s32 = (float)s64;
 #define ZKX_CFAR_CASE(A, B, C, D) \
-    if (gr == A && gc == B && rr == C && rc == D) return accurate_impl<A, B, C, D>(x, rows, columns, s32, s64, threshold, detections, stream);
+    if (gr == A && gc == B && rr == C && rc == D) return accurate_impl<A, B, C, D>(x, rows, columns, s32, s64, threshold, detections, batch, stream);
     ZKX_CFAR_CASE(2, 2, 8, 8)
     ZKX_CFAR_CASE(1, 1, 4, 4)
     ZKX_CFAR_CASE(2, 2, 4, 4)
     ZKX_CFAR_CASE(1, 1, 2, 2)
 #undef ZKX_CFAR_CASE
     const long long count = (long long)rows * columns;
-    cfar_generic_kernel<<<(unsigned)((count + 255) / 256), 256, 0, stream>>>(
+    cfar_generic_kernel<<<dim3((unsigned)((count + 255) / 256), batch), 256, 0, stream>>>(
         x, rows, columns, gr, gc, rr, rc, s64, threshold, detections);
     ZKX_LAUNCHED("cfar_generic_kernel");
     return ZKX_SUCCESS;

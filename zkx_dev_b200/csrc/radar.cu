@@ -267,6 +267,10 @@ pulse_doppler_kernel(const float2* __restrict__ x, int pulses, int samples,
     const int col = blockIdx.x * C + c;
     const bool active = col < samples;
     (void)PAD;
+    // CPI of a stacked batch
+    x += (size_t)blockIdx.y * pulses * samples;
+    if (out) out += (size_t)blockIdx.y * N * samples;
+    if (power) power += (size_t)blockIdx.y * N * samples;
     float2 v[PL::E];
 #pragma unroll
     for (int r = 0; r < PL::E; ++r) {
@@ -313,12 +317,16 @@ pulse_doppler_tma_kernel(const __grid_constant__ CUtensorMap tmap, int pulses, i
     const int c = threadIdx.x % C;
     const int t = threadIdx.x / C;
     const int col0 = blockIdx.x * C;
+    const int cpi = blockIdx.y;  // CPI of a stacked batch: rows cpi*pulses .. +pulses-1
+    if (out) out += (size_t)cpi * N * samples;
+    if (power) power += (size_t)cpi * N * samples;
     if (threadIdx.x == 0) mbar_init(bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(bar, (uint32_t)(N * C * sizeof(float2)));
 #pragma unroll
-        for (int b = 0; b < N / BOXH; ++b) tma_load_2d(sm + b * BOXH * C, &tmap, 2 * col0, b * BOXH, bar);
+        for (int b = 0; b < N / BOXH; ++b)
+            tma_load_2d(sm + b * BOXH * C, &tmap, 2 * col0, cpi * pulses + b * BOXH, bar);
     }
     const bool ok = mbar_wait_bounded(bar, 0);
     if (__syncthreads_or(!ok)) {
@@ -331,7 +339,8 @@ pulse_doppler_tma_kernel(const __grid_constant__ CUtensorMap tmap, int pulses, i
 #pragma unroll
     for (int r = 0; r < PL::E; ++r) {
         const int e = t + PL::T * r;
-        float2 a = sm[e * C + c];
+        // rows past this CPI's pulses (zero padding to nfft) may hold the next CPI's data
+        float2 a = e < pulses ? sm[e * C + c] : make_float2(0.f, 0.f);
         if (window && e < pulses) {
             const float w = __ldg(&window[e]);
             a.x *= w;
@@ -410,18 +419,19 @@ int compression_impl(const float2* x, int pulses, int samples, const float2* spe
 
 template <int N>
 int doppler_impl(const float2* x, int pulses, int samples, const float* window, float2* out,
-                 float* power, cudaStream_t s)
+                 float* power, int batch, cudaStream_t s)
 {
     if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
     using PL = FftPlan<N, elems_for(N)>;
     constexpr int C = doppler_columns(N);
-    const int blocks = (samples + C - 1) / C;
+    const dim3 blocks((samples + C - 1) / C, batch);
+    if (batch > 65535) return fail(ZKX_UNSUPPORTED_OPERATION, "pulse_doppler: more than 65535 CPIs in one batch");
     if constexpr (C == 16) {
         // TMA path: rows must be 16-byte multiples and the base 16-byte aligned
         if ((samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
             CUtensorMap map;
             constexpr int BOXH = N < 256 ? N : 256;
-            if (encode_tensor_map_2d_f32(&map, x, 2ull * samples, (uint64_t)pulses,
+            if (encode_tensor_map_2d_f32(&map, x, 2ull * samples, (uint64_t)pulses * batch,
                                          (uint64_t)samples * sizeof(float2), 32, BOXH)) {
                 const size_t smem = (size_t)N * C * sizeof(float2) + 16;
                 auto k = pulse_doppler_tma_kernel<N>;
@@ -494,10 +504,10 @@ int launch_pulse_compression(const float2* x, int pulses, int samples, int nfft,
 }
 
 int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft, const float* window,
-                         float2* out, float* power, cudaStream_t stream)
+                         float2* out, float* power, int batch, cudaStream_t stream)
 {
     if (nfft > 4096) return fail(ZKX_UNSUPPORTED_OPERATION, "pulse_doppler: nfft above 4096 is not supported");
-#define ZKX_CALL(NN) doppler_impl<NN>(x, pulses, samples, window, out, power, stream)
+#define ZKX_CALL(NN) doppler_impl<NN>(x, pulses, samples, window, out, power, batch, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
 #undef ZKX_CALL
 }

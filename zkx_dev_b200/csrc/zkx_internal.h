@@ -59,14 +59,15 @@ int launch_replica_spectrum(const float2* replica, int length, int nfft, int nor
 int launch_pulse_compression(const float2* x, int pulses, int samples, int nfft,
                              const float2* spectrum, float2* y, cudaStream_t stream);
 int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft,
-                         const float* window, float2* out, float* power, cudaStream_t stream);
+                         const float* window, float2* out, float* power, int batch,
+                         cudaStream_t stream);
 int launch_fft_rows(const float2* x, int rows, int n, int inverse, float2* y, cudaStream_t stream);
 int launch_doppler_window(int pulses, int window_kind, const float* explicit_window, float* out,
                           cudaStream_t stream);
 int launch_ca_cfar_accurate(const float* x, int rows, int columns, int guard_rows,
                             int guard_columns, int reference_rows, int reference_columns,
                             double alpha, int reference_count, float* threshold,
-                            uint8_t* detections, cudaStream_t stream);
+                            uint8_t* detections, int batch, cudaStream_t stream);
 int launch_ca_cfar_compat(const float* x, int rank, int rows, int columns, int guard_rows,
                           int guard_columns, int reference_rows, int reference_columns,
                           float alpha, int reference_count, float* cumulative, float* threshold,
