@@ -1,7 +1,7 @@
 // Complex types and the batched device FFT of the cusignal_cpp FFT backend
 // (ZKX/cusignal_cpp/include/cusignal/backends/fft/fft_interface.h:104-117, 499-536):
 // forward transforms are unnormalised, inverse transforms scale by 1/N.  Lengths are
-// powers of two up to 16384; the device calls run the B200 shared-memory FFT on the
+// powers of two up to 65536; the device calls run the B200 shared-memory FFT on the
 // legacy default stream.
 #pragma once
 

@@ -15,7 +15,8 @@
  * work is queued.  The last failure's message is available per host thread from
  * zkx_last_error().
  *
- * Transform lengths (nfft) must be powers of two from 1 to 16384.
+ * Transform lengths (nfft) must be powers of two: 1 to 65536 along range (lengths above
+ * 16384 run on clusters of two or four CTAs) and 1 to 4096 along pulses (Doppler).
  */
 #ifndef ZKX_RD_H
 #define ZKX_RD_H
@@ -118,7 +119,9 @@ ZKX_API int zkx_pulse_compression_c64_noalloc(const void* x, int num_pulses, int
                                               zkx_stream_t stream);
 
 /* The replica spectrum alone: spectrum[k] = conj(FFT(w*h/||w*h||, nfft))[k] / nfft,
- * the per-bin factor that zkx_pulse_compression_spectrum_c64 applies.  Lets callers
+ * the per-bin factor that zkx_pulse_compression_spectrum_c64 applies.  For nfft above
+ * 16384 the bins are stored in cluster order (bin k1 + R*k2 at index k1*16384 + k2,
+ * R = nfft / 16384), the order the long compression kernel consumes them in.  Lets callers
  * keep a spectrum resident per waveform (no counterpart call in the reference, which
  * recomputes it inside radartools_typed.cu:199-215). */
 ZKX_API int zkx_replica_spectrum_c64(const void* replica, int replica_length, int nfft, int normalize,
@@ -140,7 +143,7 @@ ZKX_API int zkx_pulse_doppler_c64(const void* x, int num_pulses, int samples_per
                           float* power, zkx_stream_t stream);
 
 /* Batched complex-to-complex FFT of `batch` contiguous rows of n complex64 (n a power of
- * two, 1..16384); forward unnormalised, inverse scaled by 1/n; x == y allowed.
+ * two, 1..65536); forward unnormalised, inverse scaled by 1/n; x == y allowed.
  * Replaces FFTInterface::fft_batch_device / ifft_batch_device
  * (include/cusignal/backends/fft/fft_interface.h:499-536; fft_interface.cpp:385-470). */
 ZKX_API int zkx_fft_c2c_c64(const void* x, int batch, int n, int inverse, void* y,

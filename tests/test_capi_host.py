@@ -48,6 +48,10 @@ def test_pulse_compression_validation_codes(L):
     assert lib.zkx_pulse_compression_c64(p, 2, 16, p, 4, -1, 1, 3, None, p, None) == L.INVALID_ARGUMENT
     assert lib.zkx_pulse_compression_c64(p, 2, 16, p, 4, -1, 1, 0, p, p, None) == L.INVALID_ARGUMENT
     assert lib.zkx_pulse_compression_c64(p, 2, 24, p, 4, -1, 1, 0, None, p, None) == L.UNSUPPORTED_OPERATION
+    # range transforms up to 65536 are supported; 131072 is not
+    assert lib.zkx_pulse_compression_c64(p, 2, 16, p, 4, 1 << 17, 1, 0, None, p, None) == L.UNSUPPORTED_OPERATION
+    assert b"65536" in lib.zkx_last_error()
+    assert lib.zkx_fft_c2c_c64(p, 2, 1 << 17, 0, p, None) == L.UNSUPPORTED_OPERATION
     assert lib.zkx_pulse_compression_c64(None, 2, 16, p, 4, -1, 1, 0, None, p, None) == L.INVALID_ARGUMENT
     assert lib.zkx_pulse_compression_c64(p, 1 << 16, 1 << 16, p, 4, -1, 1, 0, None, p, None) == L.INVALID_SHAPE
     assert b"pulse_compression" in lib.zkx_last_error()

@@ -12,7 +12,7 @@ using namespace zkx;
 
 namespace {
 
-constexpr int kMaxNfft = 1 << kMaxSmemFftLog;
+constexpr int kMaxNfft = 1 << 16;  // 65536 (two or four clustered CTAs above 16384)
 
 bool valid_window(int kind, const void* explicit_window)
 {
@@ -26,7 +26,7 @@ int check_transform_length(int nfft, const char* fn)
     if (nfft < 1) return fail(ZKX_INVALID_ARGUMENT, std::string(fn) + ": nfft must be positive");
     if (!is_pow2(nfft) || nfft > kMaxNfft)
         return fail(ZKX_UNSUPPORTED_OPERATION,
-                    std::string(fn) + ": nfft must be a power of two no larger than 16384");
+                    std::string(fn) + ": nfft must be a power of two no larger than 65536");
     return ZKX_SUCCESS;
 }
 

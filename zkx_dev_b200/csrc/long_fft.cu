@@ -1,0 +1,331 @@
+// Range transforms longer than one CTA's shared memory (N = 32768 and 65536) for
+// sm_100a.  N = R * M with M = 16384: the R CTAs of a thread-block cluster (R = 2 or
+// 4) each hold one M-point sub-transform in shared memory and registers (512 threads x
+// 32 values, the same plan as the single-CTA 16384-point transform), and the radix-R
+// butterflies between the sub-transforms are exchanged through distributed shared
+// memory:
+//
+//   forward (decimation in frequency):
+//     b_k1[n2]       = W_N^(n2 k1) sum_n1 x[n1 M + n2] W_R^(n1 k1)      (cross-CTA pass)
+//     X[k1 + R k2]   = sum_n2 b_k1[n2] W_M^(n2 k2)          in CTA k1   (local transform)
+//   inverse (decimation in time), CTA k1 holds Y[k1 + R k2]:
+//     z_k1[m]        = W_N^(-m k1) sum_k2 Y[k1 + R k2] W_M^(-m k2)     (local transform)
+//     y[c M + m]     = sum_k1 W_R^(-c k1) z_k1[m]                       (cross-CTA pass)
+//
+// Each cross-CTA pass splits the M positions into R slices of S = M / R: the CTA that
+// owns a slice computes the whole R-point butterfly for it and pushes every result
+// straight into the shared memory of the CTA that needs it (remote stores, which do
+// not stall the sender), so each value crosses the SM-to-SM network at most once per
+// pass and the input and output cross HBM exactly once.  Range compression keeps the
+// spectrum in "cluster order" (bin k1 + R k2 at k1 M + k2) and never reorders.
+#include <cooperative_groups.h>
+
+#include "fft_core.cuh"
+#include "window.cuh"
+#include "zkx_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace zkx {
+namespace {
+
+using SubPlan = FftPlan<1 << kMaxSmemFftLog, 32>;
+constexpr int kM = SubPlan::N;
+constexpr int kT = SubPlan::T;
+constexpr int kE = SubPlan::E;
+
+// 32-bit shared::cluster address of `p` (this CTA's shared memory) in cluster CTA `rank`.
+__device__ __forceinline__ uint32_t cluster_address(const void* p, int rank)
+{
+    const uint32_t local = (uint32_t)__cvta_generic_to_shared(p);
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank));
+    return remote;
+}
+
+__device__ __forceinline__ void store_cluster(uint32_t address, float2 v)
+{
+    asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(address), "f"(v.x), "f"(v.y)
+                 : "memory");
+}
+
+// exp(DIR * 2 pi i j / N) for N = R * M, from the FP64-generated 65536-entry table.
+template <int R, int DIR>
+__device__ __forceinline__ float2 long_twiddle(const float2* __restrict__ tw, int j)
+{
+    constexpr int LOGN = kMaxSmemFftLog + ilog2(R);
+    const float2 w = __ldg(&tw[((unsigned)j << (kTwiddleLog - LOGN)) & (kTwiddleSize - 1)]);
+    return DIR > 0 ? cconj(w) : w;
+}
+
+// Cross-CTA decimation-in-frequency pass.  CTA c owns n2 in [c S, c S + S): it reads
+// x[n1 M + n2] for every n1 through `load(index)` and stores b_k1[n2] into sm[n2] of
+// cluster CTA k1.  On return (after a cluster barrier) sm[n2] of this CTA holds its
+// own b[n2] for all n2.
+template <int R, int DIR, class Load>
+__device__ __forceinline__ void cross_dif_scatter(const cg::cluster_group& cl, float2* sm, int c,
+                                                  int t, const float2* __restrict__ tw, Load load)
+{
+    constexpr int S = kM / R, PER = S / kT;
+    uint32_t dst[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) dst[k] = cluster_address(sm, k);
+    cl.sync();  // every CTA of the cluster is running before its shared memory is written
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        const int n2 = c * S + t + kT * j;
+        float2 a[R];
+#pragma unroll
+        for (int n1 = 0; n1 < R; ++n1) a[n1] = load(n1 * kM + n2);
+        dft<R, DIR>(a);
+#pragma unroll
+        for (int k1 = 0; k1 < R; ++k1)
+            store_cluster(dst[k1] + 8u * n2, k1 ? cmul(a[k1], long_twiddle<R, DIR>(tw, n2 * k1)) : a[k1]);
+    }
+    cl.sync();  // all of this CTA's b values have arrived
+}
+
+// Cross-CTA decimation-in-time pass after the local inverse sub-transforms: v[r] of
+// CTA k1 holds z_k1[m] (before its twiddle), m = t + T r.  Slice s of every z_k1 goes
+// to CTA s, which writes y[c M + m] = scale * sum_k1 W_R^(DIR c k1) W_N^(DIR m k1) z_k1[m]
+// for its m and every c.
+template <int R, int DIR>
+__device__ __forceinline__ void cross_dit_gather(const cg::cluster_group& cl, const float2 (&v)[kE],
+                                                 float2* sm, int k1, int t,
+                                                 const float2* __restrict__ tw, float2* yr,
+                                                 float scale)
+{
+    constexpr int S = kM / R, PER = S / kT;
+    uint32_t dst[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) dst[k] = cluster_address(sm, k);
+    cl.sync();  // every CTA has finished its local transform: exchange buffers are free
+#pragma unroll
+    for (int r = 0; r < kE; ++r) {
+        const int m = t + kT * r;
+        const float2 zv = k1 ? cmul(v[r], long_twiddle<R, DIR>(tw, m * k1)) : v[r];
+        store_cluster(dst[r / PER] + 8u * (k1 * S + t + kT * (r % PER)), zv);
+    }
+    cl.sync();
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        const int mm = t + kT * j;
+        float2 a[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k) a[k] = sm[k * S + mm];
+        dft<R, DIR>(a);
+#pragma unroll
+        for (int c = 0; c < R; ++c) {
+            float2 o = a[c];
+            if (scale != 1.0f) o = make_float2(o.x * scale, o.y * scale);
+            yr[(size_t)c * kM + k1 * S + mm] = o;
+        }
+    }
+}
+
+// After a forward-ordered local transform CTA k1 holds X[k1 + R k2] in v[r]
+// (k2 = t + T r); bin k belongs to output chunk k / M, which receives it through its
+// shared memory and writes the chunk in natural order.
+template <int R>
+__device__ __forceinline__ void cross_natural_scatter(const cg::cluster_group& cl,
+                                                      const float2 (&v)[kE], float2* sm, int k1,
+                                                      int t, float2* yr, float scale)
+{
+    constexpr int S = kM / R, PER = S / kT;
+    uint32_t dst[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) dst[k] = cluster_address(sm, k);
+    cl.sync();
+#pragma unroll
+    for (int r = 0; r < kE; ++r)
+        store_cluster(dst[r / PER] + 8u * (k1 + R * (t + kT * (r % PER))), v[r]);
+    cl.sync();
+    float2* out = yr + (size_t)k1 * kM;
+#pragma unroll
+    for (int r = 0; r < kE; ++r) {
+        float2 o = sm[t + kT * r];
+        if (scale != 1.0f) o = make_float2(o.x * scale, o.y * scale);
+        out[t + kT * r] = o;
+    }
+}
+
+// v[r] = sm[t + T r], then a block barrier so the local transform may reuse sm.
+__device__ __forceinline__ void take_own(float2 (&v)[kE], const float2* sm, int t)
+{
+#pragma unroll
+    for (int r = 0; r < kE; ++r) v[r] = sm[t + kT * r];
+    __syncthreads();
+}
+
+// Replica spectrum in cluster order: spectrum[k1 M + k2] = conj(H[k1 + R k2]) / N with
+// H = FFT(w h / ||w h||, N); the FP64 norm runs over all `length` samples
+// (radartools_typed.cpp:639-648) and is recomputed by each CTA of the cluster.
+template <int R>
+__global__ void __cluster_dims__(R, 1, 1) __launch_bounds__(kT, 1)
+long_replica_kernel(const float2* __restrict__ h, int length, int normalize, int window_kind,
+                    const float* __restrict__ explicit_window, float2* __restrict__ spectrum,
+                    const float2* __restrict__ tw)
+{
+    extern __shared__ __align__(16) float2 sm[];
+    __shared__ double partial[kT];
+    const cg::cluster_group cl = cg::this_cluster();
+    const int k1 = (int)cl.block_rank();
+    const int t = threadIdx.x;
+    constexpr int N = R * kM;
+    double acc = 0.0;
+    for (int i = t; i < length; i += kT) {
+        const double w = window_value(window_kind, explicit_window, i, length);
+        const float2 hv = h[i];
+        const double re = (double)hv.x * w, im = (double)hv.y * w;
+        acc += re * re + im * im;
+    }
+    partial[t] = acc;
+    __syncthreads();
+    if (t == 0) {
+        double total = 0.0;
+        for (int i = 0; i < kT; ++i) total += partial[i];
+        partial[0] = total;
+    }
+    __syncthreads();
+    const double norm = normalize ? sqrt(partial[0]) : 1.0;
+    const float scale = (float)(1.0 / (norm * (double)N));
+    cross_dif_scatter<R, -1>(cl, sm, k1, t, tw, [&](int e) {
+        float2 val = make_float2(0.f, 0.f);
+        if (e < length) {
+            const float w = window_value(window_kind, explicit_window, e, length);
+            const float2 hv = h[e];
+            val = make_float2(hv.x * w, hv.y * w);
+        }
+        return val;
+    });
+    float2 v[kE];
+    take_own(v, sm, t);
+    fft_block<SubPlan, -1, 1>(v, sm, t, tw);
+    float2* out = spectrum + (size_t)k1 * kM;
+#pragma unroll
+    for (int r = 0; r < kE; ++r) out[t + kT * r] = make_float2(v[r].x * scale, -v[r].y * scale);
+}
+
+// One pulse per cluster: cross-CTA pass on the pulse (zero-padded/truncated to N),
+// local forward transform, product with the cluster-order spectrum, local inverse
+// transform, cross-CTA pass and store.
+template <int R>
+__global__ void __cluster_dims__(R, 1, 1) __launch_bounds__(kT, 1)
+long_compression_kernel(const float2* __restrict__ x, int samples,
+                        const float2* __restrict__ spectrum, float2* __restrict__ y,
+                        const float2* __restrict__ tw)
+{
+    extern __shared__ __align__(16) float2 sm[];
+    const cg::cluster_group cl = cg::this_cluster();
+    const int k1 = (int)cl.block_rank();
+    const int t = threadIdx.x;
+    const size_t pulse = blockIdx.x / R;
+    constexpr int N = R * kM;
+    const int avail = samples < N ? samples : N;
+    const float2* xr = x + pulse * (size_t)samples;
+    cross_dif_scatter<R, -1>(cl, sm, k1, t, tw,
+                             [&](int e) { return e < avail ? __ldcs(&xr[e]) : make_float2(0.f, 0.f); });
+    float2 v[kE];
+    take_own(v, sm, t);
+    fft_block<SubPlan, -1, 1>(v, sm, t, tw);
+    const float2* sp = spectrum + (size_t)k1 * kM;
+#pragma unroll
+    for (int r = 0; r < kE; ++r) v[r] = cmul(v[r], __ldg(&sp[t + kT * r]));
+    __syncthreads();
+    fft_block<SubPlan, 1, 1>(v, sm, t, tw);
+    cross_dit_gather<R, 1>(cl, v, sm, k1, t, tw, y + pulse * (size_t)N, 1.0f);
+}
+
+// Batched C2C rows of length N, natural order in and out; forward unnormalised,
+// inverse scaled by 1/N.  Every CTA reads its input slice before the second cluster
+// barrier and writes only after later ones, so x == y is safe.
+template <int R, int DIR>
+__global__ void __cluster_dims__(R, 1, 1) __launch_bounds__(kT, 1)
+long_fft_rows_kernel(const float2* x, float2* y, const float2* __restrict__ tw)
+{
+    extern __shared__ __align__(16) float2 sm[];
+    const cg::cluster_group cl = cg::this_cluster();
+    const int k1 = (int)cl.block_rank();
+    const int t = threadIdx.x;
+    const size_t row = blockIdx.x / R;
+    constexpr int N = R * kM;
+    const float2* xr = x + row * (size_t)N;
+    cross_dif_scatter<R, DIR>(cl, sm, k1, t, tw, [&](int e) { return xr[e]; });
+    float2 v[kE];
+    take_own(v, sm, t);
+    fft_block<SubPlan, DIR, 1>(v, sm, t, tw);
+    cross_natural_scatter<R>(cl, v, sm, k1, t, y + row * (size_t)N, DIR > 0 ? 1.0f / (float)N : 1.0f);
+}
+
+constexpr size_t kSmemBytes = (size_t)SubPlan::smem_elems() * sizeof(float2);
+
+template <class K>
+int prepare(K kernel)
+{
+    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
+    ZKX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
+    return ZKX_SUCCESS;
+}
+
+template <int R>
+int replica_long(const float2* h, int length, int normalize, int kind, const float* w,
+                 float2* spectrum, cudaStream_t s)
+{
+    auto k = long_replica_kernel<R>;
+    ZKX_TRY(prepare(k));
+    k<<<R, kT, kSmemBytes, s>>>(h, length, normalize, kind, w, spectrum, twiddle_table());
+    ZKX_LAUNCHED("long_replica_kernel");
+    return ZKX_SUCCESS;
+}
+
+template <int R>
+int compression_long(const float2* x, int pulses, int samples, const float2* spectrum, float2* y,
+                      cudaStream_t s)
+{
+    auto k = long_compression_kernel<R>;
+    ZKX_TRY(prepare(k));
+    k<<<(unsigned)pulses * R, kT, kSmemBytes, s>>>(x, samples, spectrum, y, twiddle_table());
+    ZKX_LAUNCHED("long_compression_kernel");
+    return ZKX_SUCCESS;
+}
+
+template <int R, int DIR>
+int fft_rows_long(const float2* x, int rows, float2* y, cudaStream_t s)
+{
+    auto k = long_fft_rows_kernel<R, DIR>;
+    ZKX_TRY(prepare(k));
+    k<<<(unsigned)rows * R, kT, kSmemBytes, s>>>(x, y, twiddle_table());
+    ZKX_LAUNCHED("long_fft_rows_kernel");
+    return ZKX_SUCCESS;
+}
+
+int unsupported() { return fail(ZKX_UNSUPPORTED_OPERATION, "transform length above 65536"); }
+
+}  // namespace
+
+int launch_long_replica_spectrum(const float2* replica, int length, int nfft, int normalize,
+                                 int window_kind, const float* explicit_window, float2* spectrum,
+                                 cudaStream_t stream)
+{
+    if (nfft == 2 * kM) return replica_long<2>(replica, length, normalize, window_kind, explicit_window, spectrum, stream);
+    if (nfft == 4 * kM) return replica_long<4>(replica, length, normalize, window_kind, explicit_window, spectrum, stream);
+    return unsupported();
+}
+
+int launch_long_compression(const float2* x, int pulses, int samples, int nfft,
+                            const float2* spectrum, float2* y, cudaStream_t stream)
+{
+    if (nfft == 2 * kM) return compression_long<2>(x, pulses, samples, spectrum, y, stream);
+    if (nfft == 4 * kM) return compression_long<4>(x, pulses, samples, spectrum, y, stream);
+    return unsupported();
+}
+
+int launch_long_fft_rows(const float2* x, int rows, int n, int inverse, float2* y,
+                         cudaStream_t stream)
+{
+    if (n == 2 * kM) return inverse ? fft_rows_long<2, 1>(x, rows, y, stream) : fft_rows_long<2, -1>(x, rows, y, stream);
+    if (n == 4 * kM) return inverse ? fft_rows_long<4, 1>(x, rows, y, stream) : fft_rows_long<4, -1>(x, rows, y, stream);
+    return unsupported();
+}
+
+}  // namespace zkx

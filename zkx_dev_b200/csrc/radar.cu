@@ -13,6 +13,7 @@
 
 #include "fft_core.cuh"
 #include "tma.cuh"
+#include "window.cuh"
 #include "zkx_internal.h"
 
 namespace zkx {
@@ -35,18 +36,6 @@ constexpr int rows_per_cta(int n)
     constexpr int kTarget = 128;
     const int t = n / elems_for(n);
     return t >= kTarget ? 1 : kTarget / t;
-}
-
-__device__ __forceinline__ float window_value(int kind, const float* explicit_window, int i,
-                                              int length)
-{
-    // Hann/Hamming evaluated in FP64 and rounded once (the reference evaluates the
-    // same formulas in FP32, radartools_kernels.cuh:150-160).
-    if (kind == ZKX_WINDOW_EXPLICIT_FP32 || kind == ZKX_WINDOW_EXPLICIT_FP64) return explicit_window[i];
-    if (kind == ZKX_WINDOW_NONE || length <= 1) return 1.0f;
-    const double c = cospi(2.0 * (double)i / (double)(length - 1));
-    if (kind == ZKX_WINDOW_HANN) return (float)(0.5 - 0.5 * c);
-    return (float)(0.54 - 0.46 * c);
 }
 
 // ------------------------------------------------------------ replica spectrum
@@ -490,6 +479,9 @@ int launch_replica_spectrum(const float2* replica, int length, int nfft, int nor
                             int window_kind, const float* explicit_window, float2* spectrum,
                             cudaStream_t stream)
 {
+    if (nfft > (1 << kMaxSmemFftLog))
+        return launch_long_replica_spectrum(replica, length, nfft, normalize, window_kind, explicit_window,
+                                            spectrum, stream);
 #define ZKX_CALL(NN) replica_impl<NN>(replica, length, normalize, window_kind, explicit_window, spectrum, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
 #undef ZKX_CALL
@@ -498,6 +490,8 @@ int launch_replica_spectrum(const float2* replica, int length, int nfft, int nor
 int launch_pulse_compression(const float2* x, int pulses, int samples, int nfft,
                              const float2* spectrum, float2* y, cudaStream_t stream)
 {
+    if (nfft > (1 << kMaxSmemFftLog))
+        return launch_long_compression(x, pulses, samples, nfft, spectrum, y, stream);
 #define ZKX_CALL(NN) compression_impl<NN>(x, pulses, samples, spectrum, y, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
 #undef ZKX_CALL
@@ -514,6 +508,7 @@ int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft, con
 
 int launch_fft_rows(const float2* x, int rows, int n, int inverse, float2* y, cudaStream_t stream)
 {
+    if (n > (1 << kMaxSmemFftLog)) return launch_long_fft_rows(x, rows, n, inverse, y, stream);
 #define ZKX_CALL(NN) fft_rows_impl<NN>(x, rows, inverse, y, stream)
     ZKX_DISPATCH_POW2(ilog2_host(n), ZKX_CALL)
 #undef ZKX_CALL

@@ -62,6 +62,15 @@ int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft,
                          const float* window, float2* out, float* power, int batch,
                          cudaStream_t stream);
 int launch_fft_rows(const float2* x, int rows, int n, int inverse, float2* y, cudaStream_t stream);
+// Lengths 32768 and 65536 (thread-block clusters, long_fft.cu); the spectrum of a long
+// transform is kept in cluster order (bin k1 + R k2 at k1 * 16384 + k2, R = nfft / 16384).
+int launch_long_replica_spectrum(const float2* replica, int length, int nfft, int normalize,
+                                 int window_kind, const float* explicit_window, float2* spectrum,
+                                 cudaStream_t stream);
+int launch_long_compression(const float2* x, int pulses, int samples, int nfft,
+                            const float2* spectrum, float2* y, cudaStream_t stream);
+int launch_long_fft_rows(const float2* x, int rows, int n, int inverse, float2* y,
+                         cudaStream_t stream);
 int launch_doppler_window(int pulses, int window_kind, const float* explicit_window, float* out,
                           cudaStream_t stream);
 int launch_ca_cfar_accurate(const float* x, int rows, int columns, int guard_rows,

@@ -49,7 +49,9 @@ def _complex_input(x: torch.Tensor, ndim: int, name: str) -> torch.Tensor:
 def replica_spectrum(template: torch.Tensor, nfft: int, normalize: bool = False,
                      window: WindowArg = None) -> torch.Tensor:
     """conj(FFT(w * template / ||w * template||, nfft)) / nfft, the factor the fused
-    range-compression kernel applies per bin (kept resident per waveform)."""
+    range-compression kernel applies per bin (kept resident per waveform).  For nfft
+    above 16384 the bins are stored in the library's cluster order (bin k1 + R*k2 at
+    k1*16384 + k2, R = nfft / 16384): pass the tensor back unchanged."""
     t = _complex_input(template, 1, "template")
     kind, w = _window(window, t.numel(), t.device)
     out = torch.empty(nfft, dtype=torch.complex64, device=t.device)
@@ -80,6 +82,18 @@ def pulse_compression(x: torch.Tensor, template: torch.Tensor, normalize: bool =
     L.check(L.lib().zkx_pulse_compression_c64(
         x.data_ptr(), P, N, t.data_ptr(), t.numel(), nf, int(normalize), kind, L.ptr(w),
         y.data_ptr(), L.stream_handle()))
+    return y
+
+
+def fft(x: torch.Tensor, inverse: bool = False, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Batched C2C transform of the rows of x (complex64 [rows, n], n a power of two up to
+    65536): forward unnormalised, inverse scaled by 1/n (FFTInterface::fft_batch_device /
+    ifft_batch_device).  ``out`` may be x itself."""
+    x = _complex_input(x, 2, "x")
+    rows, n = x.shape
+    y = torch.empty_like(x) if out is None else out
+    L.check(L.lib().zkx_fft_c2c_c64(x.data_ptr(), rows, n, int(bool(inverse)), y.data_ptr(),
+                                    L.stream_handle()))
     return y
 
 
