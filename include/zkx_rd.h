@@ -300,6 +300,75 @@ ZKX_API int zkx_rd_graph_create(zkx_rd_plan plan, const void* x, int batch, void
 ZKX_API int zkx_rd_graph_launch(zkx_rd_graph graph, zkx_stream_t stream);
 ZKX_API int zkx_rd_graph_destroy(zkx_rd_graph graph);
 
+/* ---------------------------------------------------------------- serving loop
+ * A continuous-batching request loop over the chain (no counterpart in the reference,
+ * whose Task1 pipeline runs one CPI per call on the default stream).  CPIs of any
+ * supported shape are submitted as they arrive; a worker thread admits them while
+ * device slots and the HBM budget allow, fuses pending CPIs of one shape and waveform
+ * into one batched launch per stage, and spreads the batches over several CUDA
+ * streams so copies and kernels of different batches overlap.  Replica spectra and
+ * Doppler windows stay resident per (shape, waveform); per-batch workspaces come from
+ * a stream-ordered memory pool and are counted against the budget. */
+
+/* Zero fields take the defaults named in the comments. */
+typedef struct {
+    int normalize;           /* replica normalisation (0/1) */
+    int range_window;        /* ZKX_WINDOW_NONE / HANN / HAMMING on the replica */
+    int doppler_window;      /* ZKX_WINDOW_NONE / HANN / HAMMING across pulses */
+    int guard_cells[2];      /* Doppler, range */
+    int reference_cells[2];  /* Doppler, range */
+    double pfa;
+    int cfar_mode;           /* ZKX_CFAR_ACCURATE or ZKX_CFAR_COMPAT */
+    int streams;             /* CUDA streams batches are spread over (4) */
+    int max_inflight;        /* batches on the device at once (2 * streams) */
+    int max_batch;           /* CPIs of one shape fused into one batch (16) */
+    double hbm_fraction;     /* budget = this fraction of the free HBM at creation (0.8) */
+    size_t budget_bytes;     /* nonzero: a lower cap on the budget */
+} zkx_rd_server_desc;
+
+/* One CPI.  x and the outputs may be host memory (page-locked for the copies to
+ * overlap) or device memory; they must stay valid until the request completes.
+ * Outputs are [P, N] (Doppler bin major, range nfft = N, Doppler nfft = P): detections
+ * is required, the others may be NULL.  Requests with the same waveform_id must pass
+ * the same replica (device memory, read when the id is first seen with this shape). */
+typedef struct {
+    int num_pulses;
+    int samples_per_pulse;   /* a power of two up to 65536 */
+    uint64_t waveform_id;
+    const void* replica;     /* complex64 [replica_length] */
+    int replica_length;
+    const void* x;           /* complex64 [P, N] */
+    uint8_t* detections;
+    float* threshold;
+    float* power;
+    void* rd;                /* complex64 */
+} zkx_rd_request;
+
+typedef struct {
+    uint64_t submitted, completed, failed, batches;
+    double mean_batch;       /* CPIs per batch */
+    double p50_us, p99_us, max_us, mean_us;  /* submit -> results in the caller's buffers */
+    double cpis_per_s;       /* completed / (last completion - first submission) */
+    size_t budget_bytes, peak_bytes, plan_bytes;
+    int plans;
+} zkx_rd_server_stats;
+
+typedef struct zkx_rd_server_s* zkx_rd_server;
+
+/* Creates the loop on the current device (starts its worker thread). */
+ZKX_API int zkx_rd_server_create(const zkx_rd_server_desc* desc, zkx_rd_server* server);
+/* Finishes every submitted request, then releases the loop. */
+ZKX_API int zkx_rd_server_destroy(zkx_rd_server server);
+/* Queues one CPI and returns at once with its ticket.  A request whose workspace
+ * alone exceeds the budget is refused with ZKX_OUT_OF_MEMORY. */
+ZKX_API int zkx_rd_submit(zkx_rd_server server, const zkx_rd_request* request, uint64_t* ticket);
+/* *done = 1 and the request's status once it has completed (the ticket is then
+ * released); *done = 0 if it is still pending after timeout_ms (0 = do not wait,
+ * negative = wait until it completes). */
+ZKX_API int zkx_rd_poll(zkx_rd_server server, uint64_t ticket, int timeout_ms, int* done);
+ZKX_API int zkx_rd_server_stats_get(zkx_rd_server server, zkx_rd_server_stats* stats);
+ZKX_API int zkx_rd_server_stats_reset(zkx_rd_server server);
+
 #ifdef __cplusplus
 }
 #endif

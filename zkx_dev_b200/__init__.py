@@ -9,7 +9,8 @@ from .radartools import (ca_cfar, cfar_alpha, fft, pulse_compression, pulse_dopp
                          replica_spectrum)
 from .filtering import firfilter, resample_poly, resample_poly_taps, upfirdn
 from .chain import ChainConfig, RangeDopplerChain
+from .serving import RdServer, ServerConfig
 
 __all__ = ["ZkxError", "ZkxValueError", "lib", "ca_cfar", "cfar_alpha", "fft", "pulse_compression",
            "pulse_doppler", "replica_spectrum", "firfilter", "resample_poly",
-           "resample_poly_taps", "upfirdn", "ChainConfig", "RangeDopplerChain"]
+           "resample_poly_taps", "upfirdn", "ChainConfig", "RangeDopplerChain", "RdServer", "ServerConfig"]

@@ -16,6 +16,7 @@ SUCCESS = 0
 INVALID_ARGUMENT = 1001
 INVALID_SHAPE = 1002
 UNSUPPORTED_OPERATION = 1004
+OUT_OF_MEMORY = 2003
 
 WINDOW_NONE, WINDOW_HANN, WINDOW_HAMMING, WINDOW_EXPLICIT_FP32, WINDOW_EXPLICIT_FP64 = range(5)
 CFAR_ACCURATE, CFAR_COMPAT = 0, 1
@@ -37,6 +38,27 @@ class RdDesc(ctypes.Structure):
                 ("doppler_nfft", _I), ("replica_length", _I), ("normalize", _I),
                 ("range_window", _I), ("doppler_window", _I), ("guard_cells", _I * 2),
                 ("reference_cells", _I * 2), ("pfa", _D), ("cfar_mode", _I)]
+
+
+class ServerDesc(ctypes.Structure):
+    _fields_ = [("normalize", _I), ("range_window", _I), ("doppler_window", _I),
+                ("guard_cells", _I * 2), ("reference_cells", _I * 2), ("pfa", _D),
+                ("cfar_mode", _I), ("streams", _I), ("max_inflight", _I), ("max_batch", _I),
+                ("hbm_fraction", _D), ("budget_bytes", ctypes.c_size_t)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("num_pulses", _I), ("samples_per_pulse", _I), ("waveform_id", ctypes.c_uint64),
+                ("replica", _P), ("replica_length", _I), ("x", _P), ("detections", _P),
+                ("threshold", _P), ("power", _P), ("rd", _P)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("mean_batch", _D),
+                ("p50_us", _D), ("p99_us", _D), ("max_us", _D), ("mean_us", _D),
+                ("cpis_per_s", _D), ("budget_bytes", ctypes.c_size_t),
+                ("peak_bytes", ctypes.c_size_t), ("plan_bytes", ctypes.c_size_t), ("plans", _I)]
 
 
 SIGNATURES = {
@@ -71,6 +93,12 @@ SIGNATURES = {
     "zkx_rd_graph_create": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, ctypes.POINTER(_P)]),
     "zkx_rd_graph_launch": (_I, [_P, _P]),
     "zkx_rd_graph_destroy": (_I, [_P]),
+    "zkx_rd_server_create": (_I, [ctypes.POINTER(ServerDesc), ctypes.POINTER(_P)]),
+    "zkx_rd_server_destroy": (_I, [_P]),
+    "zkx_rd_submit": (_I, [_P, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]),
+    "zkx_rd_poll": (_I, [_P, ctypes.c_uint64, _I, ctypes.POINTER(_I)]),
+    "zkx_rd_server_stats_get": (_I, [_P, ctypes.POINTER(ServerStats)]),
+    "zkx_rd_server_stats_reset": (_I, [_P]),
 }
 
 _lib: Optional[ctypes.CDLL] = None

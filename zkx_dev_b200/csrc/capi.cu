@@ -444,9 +444,10 @@ extern "C" int zkx_rd_plan_shape(zkx_rd_plan plan, int* range_bins, int* doppler
     return ZKX_SUCCESS;
 }
 
-extern "C" int zkx_rd_execute_batch(zkx_rd_plan p, const void* x, int batch, void* compressed,
-                                    void* rd, float* power, float* threshold, uint8_t* detections,
-                                    zkx_stream_t stream)
+namespace zkx {
+int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compressed, void* rd,
+                        float* power, float* threshold, uint8_t* detections, float* cumulative,
+                        cudaStream_t stream)
 {
     if (!p || !x || !threshold || !detections) return fail(ZKX_INVALID_ARGUMENT, "rd_execute: null pointer");
     if (batch < 1) return fail(ZKX_INVALID_SHAPE, "rd_execute: batch must be positive");
@@ -475,7 +476,8 @@ extern "C" int zkx_rd_execute_batch(zkx_rd_plan p, const void* x, int batch, voi
         }
         power = p->power;
     }
-    if (p->d.cfar_mode == ZKX_CFAR_COMPAT && p->cumulative_elems < (size_t)nd * nr)
+    if (!cumulative) cumulative = p->cumulative;
+    if (p->d.cfar_mode == ZKX_CFAR_COMPAT && !cumulative)
         return fail(ZKX_INTERNAL_ERROR, "rd_execute: compat workspace missing");
     // the CPIs of a batch are contiguous, so range compression sees batch*P pulses
     ZKX_TRY(launch_pulse_compression(static_cast<const float2*>(x), batch * P, N, nr, p->spectrum,
@@ -487,13 +489,22 @@ extern "C" int zkx_rd_execute_batch(zkx_rd_plan p, const void* x, int batch, voi
     if (p->d.cfar_mode == ZKX_CFAR_COMPAT) {
         for (int b = 0; b < batch; ++b)
             ZKX_TRY(launch_ca_cfar_compat(power + (size_t)b * nd * nr, 2, nd, nr, gd[0], gd[1], rf[0], rf[1],
-                                          (float)p->cfar.alpha, p->cfar.nref, p->cumulative,
+                                          (float)p->cfar.alpha, p->cfar.nref, cumulative,
                                           threshold + (size_t)b * nd * nr, detections + (size_t)b * nd * nr,
                                           stream));
         return ZKX_SUCCESS;
     }
     return launch_ca_cfar_accurate(power, nd, nr, gd[0], gd[1], rf[0], rf[1], p->cfar.alpha,
                                    p->cfar.nref, threshold, detections, batch, stream);
+}
+}  // namespace zkx
+
+extern "C" int zkx_rd_execute_batch(zkx_rd_plan p, const void* x, int batch, void* compressed,
+                                    void* rd, float* power, float* threshold, uint8_t* detections,
+                                    zkx_stream_t stream)
+{
+    return rd_execute_batch_ws(p, x, batch, compressed, rd, power, threshold, detections, nullptr,
+                               stream);
 }
 
 extern "C" int zkx_rd_execute(zkx_rd_plan p, const void* x, void* compressed, void* rd,

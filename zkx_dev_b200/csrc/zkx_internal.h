@@ -83,6 +83,12 @@ int launch_ca_cfar_compat(const float* x, int rank, int rows, int columns, int g
                           uint8_t* detections, cudaStream_t stream);
 int launch_fir(const float* b, int nb, const float* x, int lines, int n, const float* zi,
                float* y, float* zf, cudaStream_t stream);
+// zkx_rd_execute_batch with an explicit compat-mode integral-image workspace
+// (nd * nr floats; NULL = the plan's own), for callers that run one plan on several
+// streams at once.
+int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compressed, void* rd,
+                        float* power, float* threshold, uint8_t* detections, float* cumulative,
+                        cudaStream_t stream);
 int launch_polyphase(const float* taps, int ntaps, int up, int down, long long offset,
                      const float* x, int lines, int n, float* y, int nout, cudaStream_t stream);
 
