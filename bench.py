@@ -199,6 +199,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict:
 
     # per-stage timing (separate pass, kernels bracketed by events)
     stage_ms = {k: [] for k in ("fir", "resample_poly", "pulse_compression", "pulse_doppler", "ca_cfar")}
+    step_ms = []
     for i in range(max(3, args.steps)):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
         k = i % n_sets
@@ -221,6 +222,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict:
         torch.cuda.synchronize()
         for j, name in enumerate(stage_ms):
             stage_ms[name].append(ev[j].elapsed_time(ev[j + 1]))
+        step_ms.append(ev[0].elapsed_time(ev[5]))
 
     # timed region: K steps, device time, max over ranks
     clocks = ClockSampler(dev.index)
@@ -268,6 +270,25 @@ def run_ours(args, rank: int, world: int, dist) -> dict:
     e2e_ms = e0.elapsed_time(e1)
     clk = clocks.stop()
 
+    # per-step end-to-end latency (host buffers in, mask out), a separate bounded pass
+    e2e_step_ms = []
+    for i in range(min(args.steps, 50)):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        xin_fe.copy_(host_fe[i % n_sets], non_blocking=True)
+        xin_cube.copy_(host_cube[i % n_sets], non_blocking=True)
+        front_end(xin_fe)
+        chain(xin_cube, out)
+        host_det.copy_(out["detections"], non_blocking=True)
+        b.record(stream)
+        b.synchronize()
+        e2e_step_ms.append(a.elapsed_time(b))
+
+    # accuracy of this run's outputs against an FP64 recomputation (sampled)
+    chain(dev_cube[0], out)
+    torch.cuda.synchronize()
+    errors = fp64_errors(host_cube[0].numpy(), replica, out)
+
     if dist is not None:
         from zkx_dev_b200.replicas import max_over_ranks
         elapsed_ms, e2e_ms = max_over_ranks([elapsed_ms, e2e_ms], dist, dev)
@@ -292,7 +313,171 @@ def run_ours(args, rank: int, world: int, dist) -> dict:
         "chain_gbs": round(sum(ALG_BYTES.values()) / (elapsed_ms / args.steps * 1e-3) / 1e9, 1),
         "gpu_launches": 5 * args.steps,
         "clocks": clk,
+        "latency_ms": {"step_p50": round(percentile(step_ms, 50), 4),
+                       "step_p99": round(percentile(step_ms, 99), 4),
+                       "e2e_p50": round(percentile(e2e_step_ms, 50), 4),
+                       "e2e_p99": round(percentile(e2e_step_ms, 99), 4)},
+        "rel_err_vs_fp64": errors,
     }
+
+
+def percentile(values, q: float) -> float:
+    v = sorted(values)
+    return v[min(len(v) - 1, max(0, int(np.ceil(q / 100.0 * len(v))) - 1))]
+
+
+def hamming_f32(n: int) -> np.ndarray:
+    """The symmetric Hamming window as the kernels apply it: FP64 formula rounded to FP32."""
+    k = np.arange(n, dtype=np.float64)
+    return (0.54 - 0.46 * np.cos(2.0 * np.pi * k / (n - 1))).astype(np.float32).astype(np.float64)
+
+
+def fp64_errors(x: np.ndarray, replica: np.ndarray, out) -> dict:
+    """Relative L2 error of the chain's outputs against numpy FP64 on samples of the CPI:
+    16 pulses of the compressed cube; 64 range columns of the range-Doppler map and power
+    (computed from the GPU's compressed cube, so each stage is measured on its own input);
+    CFAR thresholds and decisions at 4096 interior cells recomputed in FP64 from the GPU's
+    power."""
+    import torch
+    rng = np.random.default_rng(7)
+    pulses, nr = x.shape
+    rows = np.sort(rng.choice(pulses, 16, replace=False))
+    h = replica.astype(np.complex128) * hamming_f32(replica.size)
+    h /= np.linalg.norm(h)
+    spec = np.conj(np.fft.fft(h, nr))
+    comp64 = np.fft.ifft(np.fft.fft(x[rows].astype(np.complex128), axis=1) * spec, axis=1)
+    comp = out["compressed"].cpu().numpy()
+    cols = np.sort(rng.choice(nr, 64, replace=False))
+    rd64 = np.fft.fft(comp[:, cols].astype(np.complex128) * hamming_f32(pulses)[:, None], axis=0)
+    rd = out["rd"][:, torch.as_tensor(cols)].cpu().numpy()
+    power = out["power"].cpu().numpy().astype(np.float64)
+    pow64 = np.abs(rd64) ** 2
+    gr, gc, tr, tc = 2, 2, 8, 8
+    nref = (2 * (gr + tr) + 1) * (2 * (gc + tc) + 1) - (2 * gr + 1) * (2 * gc + 1)
+    alpha = nref * (1e-6 ** (-1.0 / nref) - 1.0)
+    cr = rng.integers(gr + tr, pulses - gr - tr, 4096)
+    cc = rng.integers(gc + tc, nr - gc - tc, 4096)
+    thr = out["threshold"].cpu().numpy()
+    det = out["detections"].cpu().numpy()
+    t64 = np.empty(cr.size)
+    for i, (r, c) in enumerate(zip(cr, cc)):
+        outer = power[r - gr - tr:r + gr + tr + 1, c - gc - tc:c + gc + tc + 1].sum()
+        inner = power[r - gr:r + gr + 1, c - gc:c + gc + 1].sum()
+        t64[i] = alpha / nref * (outer - inner)
+    t32 = thr[cr, cc].astype(np.float64)
+
+    def rel(a, b):
+        return float(np.linalg.norm((np.asarray(a) - b).ravel()) / np.linalg.norm(b.ravel()))
+
+    return {"compressed": rel(comp[rows], comp64), "rd": rel(rd, rd64),
+            "power": rel(power[:, cols], pow64),
+            "threshold_max": float(np.max(np.abs(t32 - t64) / t64)),
+            "mask_mismatches": int(np.sum(det[cr, cc] != (power[cr, cc] > t64))),
+            "sample": "16 pulses; 64 range columns; 4096 interior CFAR cells"}
+
+
+def run_serving(dev, n_requests: int = 256, pool: int = 24, seconds: float = 2.0) -> dict:
+    """The mixed-size stream: pulses 2^U{6..10}, range 2^U{10..15}, 5-50 targets, chirp
+    length range/16, Hamming windows, CFAR guard 2x2 train 8x8 Pfa 1e-6.  A pool of `pool`
+    seeded CPIs is drawn from that distribution and `n_requests` requests are drawn from
+    the pool.  Measures (1) the plain path, one CPI per launch sequence on one stream,
+    (2) the serving loop on device-resident buffers and (3) with page-locked host
+    buffers (copies included), all submitted at once, then (4) the serving loop under
+    Poisson arrivals at 70 % of (3)'s rate for `seconds`, for its latency."""
+    import random
+    import torch
+    import zkx_dev_b200 as z
+    from zkx_dev_b200 import synth
+
+    rng = np.random.default_rng(synth.seed_for(4, 0))
+    cpis = []
+    for i in range(pool):
+        P_, N_ = int(2 ** rng.integers(6, 11)), int(2 ** rng.integers(10, 16))
+        cpis.append(synth.make_cpi(P_, N_, int(rng.integers(5, 51)), N_ // 16, synth.seed_for(4, i + 1)))
+    order = [int(rng.integers(0, pool)) for _ in range(n_requests)]
+    dev_x = [torch.as_tensor(c.x, device=dev) for c in cpis]
+    host_x = [torch.as_tensor(c.x).pin_memory() for c in cpis]
+    replicas = {}
+    for c in cpis:
+        replicas.setdefault(c.x.shape, torch.as_tensor(c.replica, device=dev))
+    cells = sum(cpis[k].x.size for k in order)
+
+    # (1) plain: one RangeDopplerChain per shape, one CPI after another on one stream
+    chains = {}
+    for c in cpis:
+        P_, N_ = c.x.shape
+        if c.x.shape not in chains:
+            ch = z.RangeDopplerChain(z.ChainConfig(P_, N_, N_ // 16), replicas[c.x.shape])
+            chains[c.x.shape] = (ch, ch.allocate_outputs(keep_compressed=False, keep_rd=False))
+    for k in range(pool):
+        ch, o = chains[cpis[k].x.shape]
+        ch.run(dev_x[k], o)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for k in order:
+        ch, o = chains[cpis[k].x.shape]
+        ch.run(dev_x[k], o)
+    b.record()
+    b.synchronize()
+    plain = n_requests / (a.elapsed_time(b) * 1e-3)
+    for ch, _ in chains.values():
+        ch.close()
+
+    def burst(server, xs, outs):
+        tickets = [server.submit(xs[k], replicas[cpis[k].x.shape], cpis[k].x.shape[0] * 100000 + cpis[k].x.shape[1],
+                                 outs[k]) for k in order]
+        for t in tickets:
+            server.wait(t)
+
+    dev_det = [torch.empty(c.x.shape, dtype=torch.uint8, device=dev) for c in cpis]
+    host_det = [torch.empty(c.x.shape, dtype=torch.uint8).pin_memory() for c in cpis]
+    res = {}
+    with z.RdServer(z.ServerConfig()) as server:
+        burst(server, dev_x, dev_det)            # builds the plans, warms the pool
+        server.reset_stats()
+        burst(server, dev_x, dev_det)
+        st_dev = server.stats()
+        server.reset_stats()
+        burst(server, host_x, host_det)
+        st_host = server.stats()
+        # Poisson arrivals at 70 % of the host-buffer burst rate
+        rate = 0.7 * st_host["cpis_per_s"]
+        server.reset_stats()
+        prng = random.Random(11)
+        tickets = []
+        t_next = time.perf_counter()
+        t_end = t_next + seconds
+        i = 0
+        while t_next < t_end:
+            while time.perf_counter() < t_next:
+                pass
+            k = order[i % n_requests]
+            tickets.append(server.submit(host_x[k], replicas[cpis[k].x.shape],
+                                         cpis[k].x.shape[0] * 100000 + cpis[k].x.shape[1], host_det[k]))
+            i += 1
+            t_next += prng.expovariate(rate)
+        for t in tickets:
+            server.wait(t)
+        st_poisson = server.stats()
+    res = {
+        "workload": (f"mixed stream: {n_requests} CPIs drawn from {pool} seeded CPIs with pulses "
+                     "2^U{6..10}, range 2^U{10..15}, chirp range/16, 5-50 targets"),
+        "cells": cells,
+        "plain_device_cpis_per_s": round(plain, 1),
+        "served_device_cpis_per_s": round(st_dev["cpis_per_s"], 1),
+        "served_vs_plain_device": round(st_dev["cpis_per_s"] / plain, 3),
+        "served_device_gbs": round(st_dev["cpis_per_s"] * cells / n_requests * 45 / 1e9, 1),
+        "served_host_cpis_per_s": round(st_host["cpis_per_s"], 1),
+        "mean_batch": round(st_dev["mean_batch"], 2),
+        "poisson_rate_cpis_per_s": round(rate, 1),
+        "poisson_requests": int(st_poisson["completed"]),
+        "poisson_p50_ms": round(st_poisson["p50_us"] / 1e3, 3),
+        "poisson_p99_ms": round(st_poisson["p99_us"] / 1e3, 3),
+        "poisson_cpis_per_s": round(st_poisson["cpis_per_s"], 1),
+        "buffers": "device: inputs and masks in HBM; host: page-locked inputs in, masks out",
+    }
+    return res
 
 
 def chain_spectrum(chain) -> int:
@@ -374,6 +559,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the mixed-stream serving measurement")
     ap.add_argument("--profile", action="store_true",
                     help="one input set, one warm-up and one step of every stage, no timing "
                          "(the command profiled under ncu)")
@@ -422,7 +608,11 @@ def main() -> None:
                 "data": "synthetic (seeded CN(0,1) + LFM targets)", "config": config,
                 "e2e": res["e2e"], "roofline": res["roofline"], "gpu_launches": res["gpu_launches"],
                 "clocks": res["clocks"], "stages_ms": res["stages_ms"], "stages_gbs": res["stages_gbs"],
-                "chain_gbs": res["chain_gbs"]}
+                "chain_gbs": res["chain_gbs"], "latency_ms": res["latency_ms"],
+                "rel_err_vs_fp64": res["rel_err_vs_fp64"]}
+        if world == 1 and not args.no_serving:
+            import torch
+            line["serving"] = run_serving(torch.device("cuda", 0))
         if world == 1 and not args.no_cpu_baseline:
             base = reference_cpu_baseline(1, 0)
             line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}

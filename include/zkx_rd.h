@@ -319,15 +319,17 @@ typedef struct {
     int reference_cells[2];  /* Doppler, range */
     double pfa;
     int cfar_mode;           /* ZKX_CFAR_ACCURATE or ZKX_CFAR_COMPAT */
-    int streams;             /* CUDA streams batches are spread over (4) */
+    int streams;             /* compute streams batches are spread over (4); copies use
+                                one copy-in and one copy-out stream besides */
     int max_inflight;        /* batches on the device at once (2 * streams) */
-    int max_batch;           /* CPIs of one shape fused into one batch (16) */
+    int max_batch;           /* CPIs of one shape fused into one batch (16, at most 64) */
     double hbm_fraction;     /* budget = this fraction of the free HBM at creation (0.8) */
     size_t budget_bytes;     /* nonzero: a lower cap on the budget */
 } zkx_rd_server_desc;
 
 /* One CPI.  x and the outputs may be host memory (page-locked for the copies to
- * overlap) or device memory; they must stay valid until the request completes.
+ * overlap) or device memory (a device-resident x is read in place); they must stay
+ * valid until the request completes.
  * Outputs are [P, N] (Doppler bin major, range nfft = N, Doppler nfft = P): detections
  * is required, the others may be NULL.  Requests with the same waveform_id must pass
  * the same replica (device memory, read when the id is first seen with this shape). */

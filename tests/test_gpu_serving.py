@@ -103,6 +103,28 @@ def test_device_buffers_and_batching(z):
         assert torch.equal(outs["threshold"].cpu(), ref["threshold"])
 
 
+def test_host_and_device_inputs_in_one_batch(z):
+    """CPIs of one shape alternate between page-locked host and device memory: a batch
+    stages the host ones and reads the device ones in place, with the same results."""
+    from zkx_dev_b200.synth import make_cpi
+    P, N = 64, 2048
+    cpis = [make_cpi(P, N, 8, 128, seed=500 + i) for i in range(8)]
+    rep = torch.as_tensor(cpis[0].replica).cuda()
+    with z.RdServer(z.ServerConfig(max_batch=8)) as server:
+        tickets = []
+        for i, c in enumerate(cpis):
+            x = torch.as_tensor(c.x).pin_memory() if i % 2 else torch.as_tensor(c.x).cuda()
+            det = torch.empty((P, N), dtype=torch.uint8).pin_memory()
+            thr = torch.empty((P, N), dtype=torch.float32, device="cuda")
+            tickets.append((server.submit(x, rep, 3, det, threshold=thr), det, thr))
+        for t, _, _ in tickets:
+            server.wait(t)
+        assert server.stats()["mean_batch"] > 1
+    for c, (_, det, thr) in zip(cpis, tickets):
+        ref = alone(z, c, P, N)
+        assert torch.equal(det, ref["detections"]) and torch.equal(thr.cpu(), ref["threshold"])
+
+
 def test_admission_within_budget(z):
     """A budget that holds one 128 x 4096 workspace (plus the plan) at a time: every
     request still completes, one per batch, and the peak stays within the budget."""

@@ -447,9 +447,10 @@ extern "C" int zkx_rd_plan_shape(zkx_rd_plan plan, int* range_bins, int* doppler
 namespace zkx {
 int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compressed, void* rd,
                         float* power, float* threshold, uint8_t* detections, float* cumulative,
-                        cudaStream_t stream)
+                        cudaStream_t stream, const void* const* table)
 {
-    if (!p || !x || !threshold || !detections) return fail(ZKX_INVALID_ARGUMENT, "rd_execute: null pointer");
+    if (!p || !(x || table) || !threshold || !detections)
+        return fail(ZKX_INVALID_ARGUMENT, "rd_execute: null pointer");
     if (batch < 1) return fail(ZKX_INVALID_SHAPE, "rd_execute: batch must be positive");
     const int P = p->d.num_pulses, N = p->d.samples_per_pulse;
     const int nr = p->range_nfft, nd = p->doppler_nfft;
@@ -480,8 +481,13 @@ int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compresse
     if (p->d.cfar_mode == ZKX_CFAR_COMPAT && !cumulative)
         return fail(ZKX_INTERNAL_ERROR, "rd_execute: compat workspace missing");
     // the CPIs of a batch are contiguous, so range compression sees batch*P pulses
-    ZKX_TRY(launch_pulse_compression(static_cast<const float2*>(x), batch * P, N, nr, p->spectrum,
-                                     static_cast<float2*>(compressed), stream));
+    if (table)
+        ZKX_TRY(launch_pulse_compression_table(reinterpret_cast<const float2* const*>(table), batch, P,
+                                               N, nr, p->spectrum, static_cast<float2*>(compressed),
+                                               stream));
+    else
+        ZKX_TRY(launch_pulse_compression(static_cast<const float2*>(x), batch * P, N, nr, p->spectrum,
+                                         static_cast<float2*>(compressed), stream));
     ZKX_TRY(launch_pulse_doppler(static_cast<const float2*>(compressed), P, nr, nd,
                                  p->doppler_window, static_cast<float2*>(rd), power, batch, stream));
     const int* gd = p->d.guard_cells;
@@ -504,7 +510,7 @@ extern "C" int zkx_rd_execute_batch(zkx_rd_plan p, const void* x, int batch, voi
                                     zkx_stream_t stream)
 {
     return rd_execute_batch_ws(p, x, batch, compressed, rd, power, threshold, detections, nullptr,
-                               stream);
+                               stream, nullptr);
 }
 
 extern "C" int zkx_rd_execute(zkx_rd_plan p, const void* x, void* compressed, void* rd,

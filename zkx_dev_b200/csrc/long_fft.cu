@@ -209,9 +209,9 @@ long_replica_kernel(const float2* __restrict__ h, int length, int normalize, int
 // One pulse per cluster: cross-CTA pass on the pulse (zero-padded/truncated to N),
 // local forward transform, product with the cluster-order spectrum, local inverse
 // transform, cross-CTA pass and store.
-template <int R>
+template <int R, class Src>
 __global__ void __cluster_dims__(R, 1, 1) __launch_bounds__(kT, 1)
-long_compression_kernel(const float2* __restrict__ x, int samples,
+long_compression_kernel(const Src src, int samples,
                         const float2* __restrict__ spectrum, float2* __restrict__ y,
                         const float2* __restrict__ tw)
 {
@@ -222,7 +222,7 @@ long_compression_kernel(const float2* __restrict__ x, int samples,
     const size_t pulse = blockIdx.x / R;
     constexpr int N = R * kM;
     const int avail = samples < N ? samples : N;
-    const float2* xr = x + pulse * (size_t)samples;
+    const float2* xr = src.row((int)pulse);
     cross_dif_scatter<R, -1>(cl, sm, k1, t, tw,
                              [&](int e) { return e < avail ? __ldcs(&xr[e]) : make_float2(0.f, 0.f); });
     float2 v[kE];
@@ -278,11 +278,11 @@ int replica_long(const float2* h, int length, int normalize, int kind, const flo
     return ZKX_SUCCESS;
 }
 
-template <int R>
-int compression_long(const float2* x, int pulses, int samples, const float2* spectrum, float2* y,
-                      cudaStream_t s)
+template <int R, class Src>
+int compression_long(const Src& x, int pulses, int samples, const float2* spectrum, float2* y,
+                     cudaStream_t s)
 {
-    auto k = long_compression_kernel<R>;
+    auto k = long_compression_kernel<R, Src>;
     ZKX_TRY(prepare(k));
     k<<<(unsigned)pulses * R, kT, kSmemBytes, s>>>(x, samples, spectrum, y, twiddle_table());
     ZKX_LAUNCHED("long_compression_kernel");
@@ -312,12 +312,25 @@ int launch_long_replica_spectrum(const float2* replica, int length, int nfft, in
     return unsupported();
 }
 
-int launch_long_compression(const float2* x, int pulses, int samples, int nfft,
-                            const float2* spectrum, float2* y, cudaStream_t stream)
+template <class Src>
+int long_compression(const Src& x, int pulses, int samples, int nfft, const float2* spectrum,
+                     float2* y, cudaStream_t stream)
 {
     if (nfft == 2 * kM) return compression_long<2>(x, pulses, samples, spectrum, y, stream);
     if (nfft == 4 * kM) return compression_long<4>(x, pulses, samples, spectrum, y, stream);
     return unsupported();
+}
+
+int launch_long_compression(const RowsContiguous& x, int pulses, int samples, int nfft,
+                            const float2* spectrum, float2* y, cudaStream_t stream)
+{
+    return long_compression(x, pulses, samples, nfft, spectrum, y, stream);
+}
+
+int launch_long_compression(const RowsTable& x, int pulses, int samples, int nfft,
+                            const float2* spectrum, float2* y, cudaStream_t stream)
+{
+    return long_compression(x, pulses, samples, nfft, spectrum, y, stream);
 }
 
 int launch_long_fft_rows(const float2* x, int rows, int n, int inverse, float2* y,

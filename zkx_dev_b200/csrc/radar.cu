@@ -12,6 +12,7 @@
 #include <algorithm>
 
 #include "fft_core.cuh"
+#include "rows.cuh"
 #include "tma.cuh"
 #include "window.cuh"
 #include "zkx_internal.h"
@@ -93,9 +94,9 @@ replica_spectrum_kernel(const float2* __restrict__ h, int length, int normalize,
 
 // G pulses per CTA; each pulse: load (zero-pad/truncate to N), forward FFT, multiply
 // by the replica spectrum, inverse FFT, store.  The cube crosses HBM once each way.
-template <int N, int G>
+template <int N, int G, class Src>
 __global__ void __launch_bounds__(G * FftPlan<N, elems_for(N)>::T)
-pulse_compression_kernel(const float2* __restrict__ x, int pulses, int samples,
+pulse_compression_kernel(const Src src, int pulses, int samples,
                          const float2* __restrict__ spectrum, float2* __restrict__ y,
                          const float2* __restrict__ tw)
 {
@@ -106,7 +107,7 @@ pulse_compression_kernel(const float2* __restrict__ x, int pulses, int samples,
     const int pulse = blockIdx.x * G + g;
     const bool active = pulse < pulses;
     float2* smg = sm + g * PL::smem_elems();
-    const float2* xr = x + (size_t)pulse * samples;
+    const float2* xr = active ? src.row(pulse) : nullptr;
     float2 v[PL::E];
 #pragma unroll
     for (int r = 0; r < PL::E; ++r) {
@@ -132,9 +133,9 @@ pulse_compression_kernel(const float2* __restrict__ x, int pulses, int samples,
 // copies of the CTA's next pulse into that buffer, so the load streams in while the
 // current results are being stored.  Pulses are read from the staged copy
 // (unpadded, element e at sm[e]), zero beyond `samples`.
-template <int N>
+template <int N, class Src>
 __global__ void __launch_bounds__(FftPlan<N, elems_for(N)>::T)
-pulse_compression_persistent_kernel(const float2* __restrict__ x, int pulses, int samples,
+pulse_compression_persistent_kernel(const Src src, int pulses, int samples,
                                     const float2* __restrict__ spectrum, float2* __restrict__ y,
                                     const float2* __restrict__ tw, int* err)
 {
@@ -147,10 +148,10 @@ pulse_compression_persistent_kernel(const float2* __restrict__ x, int pulses, in
     constexpr uint32_t kChunk = 32768;                          // bytes per bulk copy
     auto issue = [&](int pulse) {
         mbar_arrive_expect_tx(bar, bytes);
-        const char* src = reinterpret_cast<const char*>(x + (size_t)pulse * samples);
+        const char* from = reinterpret_cast<const char*>(src.row(pulse));
         char* dst = reinterpret_cast<char*>(sm);
         for (uint32_t off = 0; off < bytes; off += kChunk)
-            bulk_load_1d(dst + off, src + off, bytes - off < kChunk ? bytes - off : kChunk, bar);
+            bulk_load_1d(dst + off, from + off, bytes - off < kChunk ? bytes - off : kChunk, bar);
     };
     if (t == 0) mbar_init(bar, 1);
     __syncthreads();
@@ -372,20 +373,20 @@ int replica_impl(const float2* h, int length, int normalize, int kind, const flo
     return ZKX_SUCCESS;
 }
 
-template <int N>
-int compression_impl(const float2* x, int pulses, int samples, const float2* spectrum, float2* y,
-                     cudaStream_t s)
+template <int N, class Src>
+int compression_impl(const Src& x, bool aligned16, int pulses, int samples, const float2* spectrum,
+                     float2* y, cudaStream_t s)
 {
     if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
     using PL = FftPlan<N, elems_for(N)>;
     if constexpr (N >= 4096) {
-        // persistent bulk-copy pipeline: 16-byte aligned pulses (even length, aligned base)
-        if ((samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+        // persistent bulk-copy pipeline: 16-byte aligned pulses (even length, aligned bases)
+        if (aligned16) {
             int dev = 0, sms = 0;
             ZKX_CUDA(cudaGetDevice(&dev));
             ZKX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
             const size_t smem = (size_t)PL::smem_elems() * sizeof(float2) + 16;
-            auto k = pulse_compression_persistent_kernel<N>;
+            auto k = pulse_compression_persistent_kernel<N, Src>;
             ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             int per_sm = 0;
             ZKX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, PL::T, smem));
@@ -398,7 +399,7 @@ int compression_impl(const float2* x, int pulses, int samples, const float2* spe
     }
     constexpr int G = rows_per_cta(N);
     const size_t smem = (size_t)G * PL::smem_elems() * sizeof(float2);
-    auto k = pulse_compression_kernel<N, G>;
+    auto k = pulse_compression_kernel<N, G, Src>;
     ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int blocks = (pulses + G - 1) / G;
     k<<<blocks, G * PL::T, smem, s>>>(x, pulses, samples, spectrum, y, twiddle_table());
@@ -490,9 +491,33 @@ int launch_replica_spectrum(const float2* replica, int length, int nfft, int nor
 int launch_pulse_compression(const float2* x, int pulses, int samples, int nfft,
                              const float2* spectrum, float2* y, cudaStream_t stream)
 {
+    const RowsContiguous src{x, samples};
     if (nfft > (1 << kMaxSmemFftLog))
-        return launch_long_compression(x, pulses, samples, nfft, spectrum, y, stream);
-#define ZKX_CALL(NN) compression_impl<NN>(x, pulses, samples, spectrum, y, stream)
+        return launch_long_compression(src, pulses, samples, nfft, spectrum, y, stream);
+    const bool aligned16 = (samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+#define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, stream)
+    ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
+#undef ZKX_CALL
+}
+
+int launch_pulse_compression_table(const float2* const* cpis, int count, int pulses_per_cpi,
+                                   int samples, int nfft, const float2* spectrum, float2* y,
+                                   cudaStream_t stream)
+{
+    if (count < 1 || count > kMaxRowTable)
+        return fail(ZKX_INVALID_ARGUMENT, "pulse_compression: 1 to 64 CPIs per table launch");
+    RowsTable src{};
+    src.pulses = pulses_per_cpi;
+    src.samples = samples;
+    bool aligned16 = (samples & 1) == 0;
+    for (int i = 0; i < count; ++i) {
+        src.cpi[i] = cpis[i];
+        aligned16 = aligned16 && (reinterpret_cast<uintptr_t>(cpis[i]) & 15) == 0;
+    }
+    const int pulses = count * pulses_per_cpi;
+    if (nfft > (1 << kMaxSmemFftLog))
+        return launch_long_compression(src, pulses, samples, nfft, spectrum, y, stream);
+#define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
 #undef ZKX_CALL
 }

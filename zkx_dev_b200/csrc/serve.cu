@@ -5,22 +5,25 @@
 // oldest pending request, fuses up to max_batch pending requests of the same shape and
 // waveform with it, and admits the batch when a device slot is free (at most
 // max_inflight batches queued on the GPU) and its workspace fits the HBM budget.  A
-// batch runs on one of the server's streams:
+// batch is a three-stage pipeline over the server's streams:
 //
-//   copies of each CPI into the batch workspace (host or device source)
-//   -> zkx_rd_execute_batch kernels (one launch per stage for the whole batch)
-//   -> copies of the requested outputs to each request's buffers
-//   -> stream-ordered free of the workspace -> host callback (completion, latency)
+//   copy-in stream   workspace from the stream-ordered pool; host-resident CPIs copied
+//                    into it (device-resident CPIs are read in place)
+//   compute stream   zkx_rd_execute_batch kernels, one launch per stage for the whole
+//                    batch (range compression reads the CPIs through a pointer table)
+//   copy-out stream  the requested outputs copied to each request's buffers, the
+//                    workspace freed, then a host callback (completion, latency)
 //
-// so while one batch computes, others copy in or out on other streams.  The callback
-// returns the workspace bytes to the budget and wakes the worker, which admits the next
-// requests without waiting for the rest of the device work: requests that arrive while
-// others are on the GPU join as soon as slots and memory free up.
+// so while one batch computes, the next copies in and the previous copies out, and the
+// kernels of consecutive batches stay in order on one compute stream (a producer's
+// output is still in L2 when its consumer runs).  The callback returns the workspace
+// bytes to the budget and wakes the worker, which admits more requests without waiting
+// for the rest of the device work: requests that arrive while others are on the GPU
+// join as soon as slots and memory free up.
 //
 // Plans (replica spectrum and Doppler window, resident) are cached per (pulses,
 // samples, replica length, waveform id) for the server's lifetime; a plan is built on
-// the stream of the first batch that needs it and later batches on other streams wait
-// on its event.
+// the copy-in stream before the first batch that needs it.
 #include <algorithm>
 #include <chrono>
 #include <climits>
@@ -63,6 +66,7 @@ struct PlanEntry {
 struct Request {
     uint64_t ticket = 0;
     zkx_rd_request r{};
+    bool x_on_device = false;  // read in place by the kernels
     PlanKey key{};
     Clock::time_point submitted;
     bool done = false;
@@ -73,24 +77,25 @@ struct Request {
 constexpr size_t kAlign = 256;
 size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 
-// Workspace of one batch of `count` CPIs [P, N] (range nfft N, Doppler nfft P).
+// Workspace of one batch of `count` CPIs [P, N] (range nfft N, Doppler nfft P), of which
+// `staged` are copied in from host memory.
 struct Layout {
     size_t x = 0, compressed = 0, rd = 0, power = 0, threshold = 0, detections = 0,
            cumulative = 0, total = 0;
 };
 
-Layout batch_layout(int P, int N, int count, bool with_rd, bool compat)
+Layout batch_layout(int P, int N, int count, int staged, bool with_rd, bool compat)
 {
-    const size_t cube = (size_t)count * P * N, map = (size_t)count * P * N;
+    const size_t cells = (size_t)P * N, cube = (size_t)count * cells, map = cube;
     Layout l;
     size_t off = 0;
-    l.x = off;          off += align_up(cube * 8);
+    l.x = off;          off += align_up((size_t)staged * cells * 8);
     l.compressed = off; off += align_up(cube * 8);
     l.power = off;      off += align_up(map * 4);
     l.threshold = off;  off += align_up(map * 4);
     l.detections = off; off += align_up(map);
     l.rd = off;         off += with_rd ? align_up(map * 8) : 0;
-    l.cumulative = off; off += compat ? align_up((size_t)P * N * 4) : 0;
+    l.cumulative = off; off += compat ? align_up(cells * 4) : 0;
     l.total = off;
     return l;
 }
@@ -100,7 +105,9 @@ Layout batch_layout(int P, int N, int count, bool with_rd, bool compat)
 struct zkx_rd_server_s {
     zkx_rd_server_desc d{};
     int device = 0;
-    std::vector<cudaStream_t> streams;
+    std::vector<cudaStream_t> streams;  // compute streams
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    std::vector<cudaEvent_t> free_events;  // reusable; returned by completion callbacks
     cudaMemPool_t pool = nullptr;
     size_t budget = 0, in_use = 0, peak = 0, plan_bytes = 0;
 
@@ -129,6 +136,8 @@ struct Batch {
     std::vector<Request*> reqs;
     size_t bytes = 0;
     bool with_rd = false;  // some request of the batch wants the complex map
+    int staged = 0;        // host-resident CPIs copied into the workspace
+    cudaEvent_t in = nullptr, done = nullptr;
 };
 
 void finish_requests(zkx_rd_server_s* s, const std::vector<Request*>& reqs, int status,
@@ -160,6 +169,8 @@ void CUDART_CB batch_done(void* arg)
         finish_requests(s, b->reqs, ZKX_SUCCESS, std::string(), now);
         s->in_use -= b->bytes;
         --s->inflight;
+        s->free_events.push_back(b->in);
+        s->free_events.push_back(b->done);
     }
     s->work_cv.notify_all();
     s->done_cv.notify_all();
@@ -198,47 +209,86 @@ int make_plan(zkx_rd_server_s* s, const Request& r, cudaStream_t stream, PlanEnt
     return ZKX_SUCCESS;
 }
 
-// Queues one batch on `stream`; on success the batch is owned by the stream callback.
+// Queues one batch on the three pipeline streams; on success the batch is owned by the
+// copy-out stream's callback.
 int issue_batch(zkx_rd_server_s* s, const PlanEntry& pe, Batch* b, const Layout& l,
-                cudaStream_t stream)
+                cudaStream_t compute)
 {
     const Request& head = *b->reqs.front();
     const int P = head.r.num_pulses, N = head.r.samples_per_pulse;
     const size_t cube = (size_t)P * N, map = (size_t)pe.doppler_bins * pe.range_bins;
     const int count = (int)b->reqs.size();
     char* ws = nullptr;
-    ZKX_CUDA(cudaStreamWaitEvent(stream, pe.ready, 0));
-    ZKX_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), l.total, s->pool, stream));
+    ZKX_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), l.total, s->pool, s->copy_in));
     auto release = [&](int rc) {
-        cudaFreeAsync(ws, stream);
+        cudaFreeAsync(ws, s->copy_in);
         return rc;
     };
-    float2* x = reinterpret_cast<float2*>(ws + l.x);
+    const void* table[kMaxRowTable];
+    float2* staged = reinterpret_cast<float2*>(ws + l.x);
+    int slot = 0;
     for (int i = 0; i < count; ++i) {
-        cudaError_t e = cudaMemcpyAsync(x + i * cube, b->reqs[i]->r.x, cube * sizeof(float2),
-                                        cudaMemcpyDefault, stream);
+        const Request& q = *b->reqs[i];
+        if (q.x_on_device) {
+            table[i] = q.r.x;
+            continue;
+        }
+        float2* dst = staged + (size_t)slot++ * cube;
+        cudaError_t e = cudaMemcpyAsync(dst, q.r.x, cube * sizeof(float2), cudaMemcpyDefault, s->copy_in);
         if (e != cudaSuccess) return release(cuda_status(e, "serving input copy"));
+        table[i] = dst;
     }
+    cudaError_t e = cudaEventRecord(b->in, s->copy_in);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(compute, b->in, 0);
+    if (e != cudaSuccess) return release(cuda_status(e, "serving pipeline event"));
     float2* rd = b->with_rd ? reinterpret_cast<float2*>(ws + l.rd) : nullptr;
     float* power = reinterpret_cast<float*>(ws + l.power);
     float* thr = reinterpret_cast<float*>(ws + l.threshold);
     uint8_t* det = reinterpret_cast<uint8_t*>(ws + l.detections);
     float* cum = s->d.cfar_mode == ZKX_CFAR_COMPAT ? reinterpret_cast<float*>(ws + l.cumulative) : nullptr;
-    int rc = rd_execute_batch_ws(pe.plan, x, count, ws + l.compressed, rd, power, thr, det, cum, stream);
-    if (rc != ZKX_SUCCESS) return release(rc);
+    // from here on the workspace is in use on the compute stream: a failure frees it
+    // after that stream's queued work
+    auto release_after_compute = [&](int rc) {
+        if (cudaEventRecord(b->done, compute) != cudaSuccess ||
+            cudaStreamWaitEvent(s->copy_in, b->done, 0) != cudaSuccess)
+            cudaStreamSynchronize(compute);
+        cudaFreeAsync(ws, s->copy_in);
+        return rc;
+    };
+    int rc = rd_execute_batch_ws(pe.plan, nullptr, count, ws + l.compressed, rd, power, thr, det, cum,
+                                 compute, table);
+    if (rc != ZKX_SUCCESS) return release_after_compute(rc);
+    e = cudaEventRecord(b->done, compute);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s->copy_out, b->done, 0);
+    if (e != cudaSuccess) return release_after_compute(cuda_status(e, "serving pipeline event"));
     for (int i = 0; i < count; ++i) {
         const zkx_rd_request& q = b->reqs[i]->r;
-        cudaError_t e = cudaMemcpyAsync(q.detections, det + i * map, map, cudaMemcpyDefault, stream);
+        e = cudaMemcpyAsync(q.detections, det + i * map, map, cudaMemcpyDefault, s->copy_out);
         if (e == cudaSuccess && q.threshold)
-            e = cudaMemcpyAsync(q.threshold, thr + i * map, map * 4, cudaMemcpyDefault, stream);
+            e = cudaMemcpyAsync(q.threshold, thr + i * map, map * 4, cudaMemcpyDefault, s->copy_out);
         if (e == cudaSuccess && q.power)
-            e = cudaMemcpyAsync(q.power, power + i * map, map * 4, cudaMemcpyDefault, stream);
+            e = cudaMemcpyAsync(q.power, power + i * map, map * 4, cudaMemcpyDefault, s->copy_out);
         if (e == cudaSuccess && q.rd)
-            e = cudaMemcpyAsync(q.rd, rd + i * map, map * 8, cudaMemcpyDefault, stream);
-        if (e != cudaSuccess) return release(cuda_status(e, "serving output copy"));
+            e = cudaMemcpyAsync(q.rd, rd + i * map, map * 8, cudaMemcpyDefault, s->copy_out);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(ws, s->copy_out);
+            return cuda_status(e, "serving output copy");
+        }
     }
-    ZKX_CUDA(cudaFreeAsync(ws, stream));
-    ZKX_CUDA(cudaLaunchHostFunc(stream, batch_done, b));
+    ZKX_CUDA(cudaFreeAsync(ws, s->copy_out));
+    ZKX_CUDA(cudaLaunchHostFunc(s->copy_out, batch_done, b));
+    return ZKX_SUCCESS;
+}
+
+// An event from the free list (or a new one); called by the worker with the lock held.
+int take_event(zkx_rd_server_s* s, cudaEvent_t* out)
+{
+    if (!s->free_events.empty()) {
+        *out = s->free_events.back();
+        s->free_events.pop_back();
+        return ZKX_SUCCESS;
+    }
+    ZKX_CUDA(cudaEventCreateWithFlags(out, cudaEventDisableTiming));
     return ZKX_SUCCESS;
 }
 
@@ -263,7 +313,8 @@ void worker_main(zkx_rd_server_s* s)
             PlanEntry pe;
             Request copy = *head;
             lk.unlock();
-            const int rc = make_plan(s, copy, stream, &pe);
+            // built on the copy-in stream, which every batch passes through first
+            const int rc = make_plan(s, copy, s->copy_in, &pe);
             const std::string msg = rc == ZKX_SUCCESS ? std::string() : std::string(zkx_last_error());
             lk.lock();
             if (rc != ZKX_SUCCESS) {
@@ -290,15 +341,18 @@ void worker_main(zkx_rd_server_s* s)
         // the oldest request and the next pending ones of its key, while they fit
         std::vector<Request*> group;
         bool with_rd = false;
+        int staged = 0;
         Layout l{};
         for (Request* q : s->pending) {
             if ((int)group.size() >= s->d.max_batch) break;
             if (!(q->key == head->key)) continue;
+            const int st = staged + (q->x_on_device ? 0 : 1);
             const Layout trial = batch_layout(head->r.num_pulses, head->r.samples_per_pulse,
-                                              (int)group.size() + 1, with_rd || q->r.rd, compat);
+                                              (int)group.size() + 1, st, with_rd || q->r.rd, compat);
             if (s->in_use + s->plan_bytes + trial.total > s->budget) break;
             group.push_back(q);
             with_rd = with_rd || q->r.rd;
+            staged = st;
             l = trial;
         }
         if (group.empty()) {
@@ -325,14 +379,19 @@ void worker_main(zkx_rd_server_s* s)
         b->reqs = group;
         b->bytes = l.total;
         b->with_rd = with_rd;
+        b->staged = staged;
+        int rc = take_event(s, &b->in);
+        if (rc == ZKX_SUCCESS) rc = take_event(s, &b->done);
         lk.unlock();
-        const int rc = issue_batch(s, pe, b, l, stream);
+        if (rc == ZKX_SUCCESS) rc = issue_batch(s, pe, b, l, stream);
         const std::string msg = rc == ZKX_SUCCESS ? std::string() : std::string(zkx_last_error());
         lk.lock();
         if (rc != ZKX_SUCCESS) {
             finish_requests(s, b->reqs, rc, msg, Clock::now());
             s->in_use -= b->bytes;
             --s->inflight;
+            if (b->in) s->free_events.push_back(b->in);
+            if (b->done) s->free_events.push_back(b->done);
             delete b;
             s->done_cv.notify_all();
         }
@@ -365,8 +424,9 @@ extern "C" int zkx_rd_server_create(const zkx_rd_server_desc* desc, zkx_rd_serve
     if (d.max_inflight <= 0) d.max_inflight = 2 * d.streams;
     if (d.max_batch <= 0) d.max_batch = 16;
     if (d.hbm_fraction <= 0) d.hbm_fraction = 0.8;
-    if (d.hbm_fraction > 1 || d.streams > 64)
-        return fail(ZKX_INVALID_ARGUMENT, "rd_server_create: hbm_fraction must be <= 1 and streams <= 64");
+    if (d.hbm_fraction > 1 || d.streams > 64 || d.max_batch > kMaxRowTable)
+        return fail(ZKX_INVALID_ARGUMENT,
+                    "rd_server_create: hbm_fraction <= 1, streams <= 64 and max_batch <= 64 required");
     const bool windows_ok = d.range_window >= ZKX_WINDOW_NONE && d.range_window <= ZKX_WINDOW_HAMMING &&
                             d.doppler_window >= ZKX_WINDOW_NONE && d.doppler_window <= ZKX_WINDOW_HAMMING;
     if (!windows_ok) return fail(ZKX_INVALID_ARGUMENT, "rd_server_create: windows must be none, hann or hamming");
@@ -377,6 +437,8 @@ extern "C" int zkx_rd_server_create(const zkx_rd_server_desc* desc, zkx_rd_serve
     s->d = d;
     auto cleanup = [&](int rc) {
         for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+        if (s->copy_in) cudaStreamDestroy(s->copy_in);
+        if (s->copy_out) cudaStreamDestroy(s->copy_out);
         if (s->pool) cudaMemPoolDestroy(s->pool);
         delete s;
         return rc;
@@ -402,6 +464,9 @@ extern "C" int zkx_rd_server_create(const zkx_rd_server_desc* desc, zkx_rd_serve
         if (e != cudaSuccess) return cleanup(cuda_status(e, "rd_server_create: stream"));
         s->streams.push_back(st);
     }
+    e = cudaStreamCreateWithFlags(&s->copy_in, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_out, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cleanup(cuda_status(e, "rd_server_create: stream"));
     s->worker = std::thread(worker_main, s);
     *out = s;
     return ZKX_SUCCESS;
@@ -416,10 +481,13 @@ extern "C" int zkx_rd_server_destroy(zkx_rd_server s)
     }
     s->work_cv.notify_all();
     if (s->worker.joinable()) s->worker.join();
-    for (cudaStream_t st : s->streams) {
-        cudaStreamSynchronize(st);
-        cudaStreamDestroy(st);
-    }
+    for (cudaStream_t st : s->streams) cudaStreamSynchronize(st);
+    cudaStreamSynchronize(s->copy_in);
+    cudaStreamSynchronize(s->copy_out);
+    for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+    cudaStreamDestroy(s->copy_in);
+    cudaStreamDestroy(s->copy_out);
+    for (cudaEvent_t ev : s->free_events) cudaEventDestroy(ev);
     for (auto& kv : s->plans) {
         cudaEventDestroy(kv.second.ready);
         zkx_rd_plan_destroy(kv.second.plan);
@@ -434,10 +502,15 @@ extern "C" int zkx_rd_submit(zkx_rd_server s, const zkx_rd_request* r, uint64_t*
 {
     if (!s || !ticket) return fail(ZKX_INVALID_ARGUMENT, "rd_submit: null pointer");
     ZKX_TRY(validate_request(r));
-    const Layout one = batch_layout(r->num_pulses, r->samples_per_pulse, 1, r->rd != nullptr,
-                                    s->d.cfar_mode == ZKX_CFAR_COMPAT);
+    cudaPointerAttributes attr{};
+    const cudaError_t pe = cudaPointerGetAttributes(&attr, r->x);
+    if (pe != cudaSuccess) return cuda_status(pe, "rd_submit: input pointer");
+    const bool on_device = attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+    const Layout one = batch_layout(r->num_pulses, r->samples_per_pulse, 1, on_device ? 0 : 1,
+                                    r->rd != nullptr, s->d.cfar_mode == ZKX_CFAR_COMPAT);
     auto* q = new Request;
     q->r = *r;
+    q->x_on_device = on_device;
     q->key = PlanKey{r->num_pulses, r->samples_per_pulse, r->replica_length, r->waveform_id};
     {
         std::lock_guard<std::mutex> lk(s->mu);

@@ -10,6 +10,7 @@
 #include <string>
 
 #include "../../include/zkx_rd.h"
+#include "rows.cuh"
 
 namespace zkx {
 
@@ -67,8 +68,15 @@ int launch_fft_rows(const float2* x, int rows, int n, int inverse, float2* y, cu
 int launch_long_replica_spectrum(const float2* replica, int length, int nfft, int normalize,
                                  int window_kind, const float* explicit_window, float2* spectrum,
                                  cudaStream_t stream);
-int launch_long_compression(const float2* x, int pulses, int samples, int nfft,
+int launch_long_compression(const RowsContiguous& x, int pulses, int samples, int nfft,
                             const float2* spectrum, float2* y, cudaStream_t stream);
+int launch_long_compression(const RowsTable& x, int pulses, int samples, int nfft,
+                            const float2* spectrum, float2* y, cudaStream_t stream);
+// Range compression of `count` CPIs [pulses_per_cpi, samples] read in place from
+// separate buffers (count <= kMaxRowTable); y is [count * pulses_per_cpi, nfft].
+int launch_pulse_compression_table(const float2* const* cpis, int count, int pulses_per_cpi,
+                                   int samples, int nfft, const float2* spectrum, float2* y,
+                                   cudaStream_t stream);
 int launch_long_fft_rows(const float2* x, int rows, int n, int inverse, float2* y,
                          cudaStream_t stream);
 int launch_doppler_window(int pulses, int window_kind, const float* explicit_window, float* out,
@@ -85,10 +93,11 @@ int launch_fir(const float* b, int nb, const float* x, int lines, int n, const f
                float* y, float* zf, cudaStream_t stream);
 // zkx_rd_execute_batch with an explicit compat-mode integral-image workspace
 // (nd * nr floats; NULL = the plan's own), for callers that run one plan on several
-// streams at once.
+// streams at once.  With a non-NULL `table` (batch <= kMaxRowTable entries) CPI b is
+// read in place from table[b] and x is ignored.
 int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compressed, void* rd,
                         float* power, float* threshold, uint8_t* detections, float* cumulative,
-                        cudaStream_t stream);
+                        cudaStream_t stream, const void* const* table = nullptr);
 int launch_polyphase(const float* taps, int ntaps, int up, int down, long long offset,
                      const float* x, int lines, int n, float* y, int nout, cudaStream_t stream);
 
