@@ -77,6 +77,17 @@ enum {
     ZKX_CFAR_COMPAT = 1
 };
 
+/* DFT arithmetic of range compression. */
+enum {
+    ZKX_PRECISION_FP32 = 0,     /* FP32 shared-memory FFT (all lengths) */
+    /* The DFT passes as tcgen05 tensor-core GEMMs on split hi + lo operands accumulated in
+     * FP32 (nfft 4096, 8192 or 16384): hi + lo FP16 with per-pulse power-of-two range
+     * scaling (error close to FP32), or hi + lo BF16 (no scaling, about 16 significant
+     * bits per operand). */
+    ZKX_PRECISION_TC_F16 = 1,
+    ZKX_PRECISION_TC_BF16 = 2
+};
+
 ZKX_API const char* zkx_last_error(void);
 ZKX_API const char* zkx_version(void);
 
@@ -132,6 +143,13 @@ ZKX_API int zkx_replica_spectrum_c64(const void* replica, int replica_length, in
 ZKX_API int zkx_pulse_compression_spectrum_c64(const void* x, int num_pulses, int samples_per_pulse,
                                        int nfft, const void* spectrum, void* y,
                                        zkx_stream_t stream);
+
+/* zkx_pulse_compression_spectrum_c64 with a chosen DFT arithmetic (ZKX_PRECISION_*); the
+ * spectrum is the natural-order one of zkx_replica_spectrum_c64.  No counterpart in the
+ * reference (its compression is FP32 only). */
+ZKX_API int zkx_pulse_compression_spectrum_ex_c64(const void* x, int num_pulses, int samples_per_pulse,
+                                                  int nfft, const void* spectrum, int precision,
+                                                  void* y, zkx_stream_t stream);
 
 /* pulse_doppler: out[k, n] = sum_p w[p] x[p, n] exp(-2 pi i k p / nfft), nfft = -1 means
  * num_pulses; optional power[k, n] = |out[k, n]|^2 (NULL to skip; out may also be NULL
@@ -260,6 +278,7 @@ typedef struct {
     int reference_cells[2];  /* Doppler, range */
     double pfa;
     int cfar_mode;           /* ZKX_CFAR_ACCURATE or ZKX_CFAR_COMPAT */
+    int precision;           /* ZKX_PRECISION_* of range compression (0 = FP32) */
 } zkx_rd_desc;
 
 typedef struct zkx_rd_plan_s* zkx_rd_plan;

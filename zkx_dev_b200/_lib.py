@@ -20,6 +20,7 @@ OUT_OF_MEMORY = 2003
 
 WINDOW_NONE, WINDOW_HANN, WINDOW_HAMMING, WINDOW_EXPLICIT_FP32, WINDOW_EXPLICIT_FP64 = range(5)
 CFAR_ACCURATE, CFAR_COMPAT = 0, 1
+PRECISION_FP32, PRECISION_TC_F16, PRECISION_TC_BF16 = 0, 1, 2
 
 # Every symbol the header declares, with its ctypes signature.
 _P = ctypes.c_void_p
@@ -37,7 +38,7 @@ class RdDesc(ctypes.Structure):
     _fields_ = [("num_pulses", _I), ("samples_per_pulse", _I), ("range_nfft", _I),
                 ("doppler_nfft", _I), ("replica_length", _I), ("normalize", _I),
                 ("range_window", _I), ("doppler_window", _I), ("guard_cells", _I * 2),
-                ("reference_cells", _I * 2), ("pfa", _D), ("cfar_mode", _I)]
+                ("reference_cells", _I * 2), ("pfa", _D), ("cfar_mode", _I), ("precision", _I)]
 
 
 class ServerDesc(ctypes.Structure):
@@ -69,6 +70,7 @@ SIGNATURES = {
     "zkx_pulse_compression_c64_noalloc": (_I, [_P, _I, _I, _P, _I, _I, _I, _I, _P, _P, _P]),
     "zkx_replica_spectrum_c64": (_I, [_P, _I, _I, _I, _I, _P, _P, _P]),
     "zkx_pulse_compression_spectrum_c64": (_I, [_P, _I, _I, _I, _P, _P, _P]),
+    "zkx_pulse_compression_spectrum_ex_c64": (_I, [_P, _I, _I, _I, _P, _I, _P, _P]),
     "zkx_pulse_doppler_c64": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, _P]),
     "zkx_fft_c2c_c64": (_I, [_P, _I, _I, _I, _P, _P]),
     "zkx_cfar_alpha": (_I, [_D, _I, ctypes.POINTER(_D)]),

@@ -31,6 +31,7 @@ class ChainConfig:
     reference_cells: Sequence[int] = (8, 8)
     pfa: float = 1e-6
     cfar_mode: str = "accurate"
+    precision: str = "fp32"   # range compression: "fp32", "tc_f16" or "tc_bf16"
 
 
 class RangeDopplerChain:
@@ -57,6 +58,8 @@ class RangeDopplerChain:
         d.reference_cells[0], d.reference_cells[1] = cfg.reference_cells
         d.pfa = cfg.pfa
         d.cfar_mode = {"accurate": L.CFAR_ACCURATE, "compat": L.CFAR_COMPAT}[cfg.cfar_mode]
+        d.precision = {"fp32": L.PRECISION_FP32, "tc_f16": L.PRECISION_TC_F16,
+                       "tc_bf16": L.PRECISION_TC_BF16}[cfg.precision]
         self._keep = (replica, rw, dw)
         h = ctypes.c_void_p()
         L.check(L.lib().zkx_rd_plan_create(ctypes.byref(d), replica.data_ptr(), L.ptr(rw),

@@ -108,6 +108,27 @@ extern "C" int zkx_pulse_compression_spectrum_c64(const void* x, int P, int N, i
                                     stream);
 }
 
+extern "C" int zkx_pulse_compression_spectrum_ex_c64(const void* x, int P, int N, int nfft,
+                                                     const void* spectrum, int precision, void* y,
+                                                     zkx_stream_t stream)
+{
+    if (precision == ZKX_PRECISION_FP32)
+        return zkx_pulse_compression_spectrum_c64(x, P, N, nfft, spectrum, y, stream);
+    if (nfft == -1) nfft = N;
+    if (precision != ZKX_PRECISION_TC_F16 && precision != ZKX_PRECISION_TC_BF16)
+        return fail(ZKX_INVALID_ARGUMENT, "pulse_compression: unknown precision");
+    ZKX_TRY(check_radar_shape(P, N, "pulse_compression"));
+    ZKX_TRY(check_radar_shape(P, nfft, "pulse_compression"));
+    if (!x || !spectrum || !y) return fail(ZKX_INVALID_ARGUMENT, "pulse_compression: null pointer");
+    if (nfft != 4096 && nfft != 8192 && nfft != 16384)
+        return fail(ZKX_UNSUPPORTED_OPERATION,
+                    "pulse_compression: tensor-core precision needs nfft 4096, 8192 or 16384");
+    ZKX_TRY(ensure_device_ready());
+    return launch_pulse_compression_tc(static_cast<const float2*>(x), P, N, nfft,
+                                       static_cast<const float2*>(spectrum), static_cast<float2*>(y),
+                                       precision, stream);
+}
+
 extern "C" int zkx_pulse_compression_c64(const void* x, int P, int N, const void* replica, int L,
                                          int nfft, int normalize, int kind, const float* w,
                                          void* y, zkx_stream_t stream)
@@ -394,6 +415,12 @@ extern "C" int zkx_rd_plan_create(const zkx_rd_desc* d, const void* replica,
     if (!valid_window(d->doppler_window, doppler_window))
         return fail(ZKX_INVALID_ARGUMENT, "pulse_doppler window is invalid");
     ZKX_TRY(check_transform_length(nd, "pulse_doppler"));
+    if (d->precision != ZKX_PRECISION_FP32 && d->precision != ZKX_PRECISION_TC_F16 &&
+        d->precision != ZKX_PRECISION_TC_BF16)
+        return fail(ZKX_INVALID_ARGUMENT, "rd_plan: unknown precision");
+    if (d->precision != ZKX_PRECISION_FP32 && nr != 4096 && nr != 8192 && nr != 16384)
+        return fail(ZKX_UNSUPPORTED_OPERATION,
+                    "rd_plan: tensor-core precision needs a range nfft of 4096, 8192 or 16384");
     if (d->cfar_mode != ZKX_CFAR_ACCURATE && d->cfar_mode != ZKX_CFAR_COMPAT)
         return fail(ZKX_INVALID_ARGUMENT, "rd_plan: unknown CFAR mode");
     CfarGeometry g;
@@ -481,7 +508,11 @@ int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compresse
     if (p->d.cfar_mode == ZKX_CFAR_COMPAT && !cumulative)
         return fail(ZKX_INTERNAL_ERROR, "rd_execute: compat workspace missing");
     // the CPIs of a batch are contiguous, so range compression sees batch*P pulses
-    if (table)
+    if (p->d.precision != ZKX_PRECISION_FP32) {
+        if (table) return fail(ZKX_UNSUPPORTED_OPERATION, "rd_execute: tensor-core plans take contiguous batches");
+        ZKX_TRY(launch_pulse_compression_tc(static_cast<const float2*>(x), batch * P, N, nr, p->spectrum,
+                                            static_cast<float2*>(compressed), p->d.precision, stream));
+    } else if (table)
         ZKX_TRY(launch_pulse_compression_table(reinterpret_cast<const float2* const*>(table), batch, P,
                                                N, nr, p->spectrum, static_cast<float2*>(compressed),
                                                stream));

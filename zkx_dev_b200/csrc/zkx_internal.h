@@ -59,6 +59,10 @@ int launch_replica_spectrum(const float2* replica, int length, int nfft, int nor
                             cudaStream_t stream);
 int launch_pulse_compression(const float2* x, int pulses, int samples, int nfft,
                              const float2* spectrum, float2* y, cudaStream_t stream);
+// Tensor-core compression (tc_dft.cu): nfft 4096, 8192, 16384; natural-order spectrum.
+int launch_pulse_compression_tc(const float2* x, int pulses, int samples, int nfft,
+                                const float2* spectrum, float2* y, int precision,
+                                cudaStream_t stream);
 int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft,
                          const float* window, float2* out, float* power, int batch,
                          cudaStream_t stream);
