@@ -1,5 +1,5 @@
 // cusignal_cpp radar tools on the range-Doppler chain -- pulse_compression,
-// pulse_doppler, ca_cfar, cfar_alpha -- with the signatures of
+// pulse_doppler, ca_cfar, cfar_alpha, ambgfun -- with the signatures of
 // ZKX/cusignal_cpp/include/cusignal/operators/radartools/radartools_typed.h (39-94,
 // 154-311), implemented over libzkx_rd.so on the legacy default stream.  T is one of
 // float, __half, int32_t, int16_t, int8_t (converted to FP32 on the device first).
@@ -21,6 +21,35 @@
 #include <vector>
 
 namespace cusignal {
+
+// radartools_typed.h:10-37
+enum class AmbgfunCut { two_dimensional, delay, doppler };
+enum class AmbgfunOutputDtype { fp32, fp64 };
+
+struct AmbgfunOptions {
+    double fs = 1.0;
+    double prf = 1.0;
+    AmbgfunCut cut = AmbgfunCut::two_dimensional;
+    double cut_value = 0.0;
+    // empty: one-dimensional input; otherwise the logical shape, whose first extent is the
+    // signal length (only the 2-D cut accepts more than one extent)
+    std::vector<int> input_shape;
+    std::vector<int> reference_shape;
+};
+
+struct AmbgfunCpuResult {
+    AmbgfunOutputDtype dtype{AmbgfunOutputDtype::fp32};
+    std::vector<float> fp32;
+    std::vector<double> fp64;
+    std::vector<int> shape;
+};
+
+struct AmbgfunDeviceResult {
+    AmbgfunOutputDtype dtype{AmbgfunOutputDtype::fp32};
+    DeviceArray<float> fp32;
+    DeviceArray<double> fp64;
+    std::vector<int> shape;
+};
 
 enum class CfarDetection : std::uint8_t { no = 0, yes = 1 };
 
@@ -129,7 +158,70 @@ inline const float* window_pointer(RadarWindowKind kind, const DeviceArray<float
     return w ? w->data() : nullptr;
 }
 
+// radartools_typed.cpp:87-106: the first extent of a logical shape that must cover the data
+inline int ambgfun_first_extent(std::size_t count, const std::vector<int>& shape, const char* label)
+{
+    if (count > static_cast<std::size_t>(std::numeric_limits<int>::max()))
+        throw std::invalid_argument(std::string("ambgfun ") + label + " length exceeds int capacity");
+    if (shape.empty()) return static_cast<int>(count);
+    std::size_t product = 1;
+    for (const int extent : shape) {
+        if (extent < 1) throw std::invalid_argument(std::string("ambgfun ") + label + " shape");
+        if (product > count / static_cast<std::size_t>(extent))
+            throw std::invalid_argument(std::string("ambgfun ") + label + " shape product");
+        product *= static_cast<std::size_t>(extent);
+    }
+    if (product != count) throw std::invalid_argument(std::string("ambgfun ") + label + " data/shape mismatch");
+    return shape.front();
+}
+
 }  // namespace detail
+
+/// Normalised ambiguity function and its delay / Doppler cuts (radartools_typed.h:97-137).
+/// Output dtype: FP32 for the 2-D cut of float or __half input, FP64 storage otherwise.
+template <class T>
+void ambgfun_device(const DeviceArray<TypedComplex<T>>& x, AmbgfunDeviceResult& output,
+                    const AmbgfunOptions& options = {}, const DeviceArray<TypedComplex<T>>* y = nullptr)
+{
+    // radartools_typed.cpp:74-85, 108-124: cut, fs and rank rules
+    const int cut = static_cast<int>(options.cut);
+    if (cut < 0 || cut > 2) throw std::invalid_argument("ambgfun cut is invalid");
+    if (cut != 0 && options.fs == 0.0)
+        throw std::invalid_argument("ambgfun fs must be nonzero for one-dimensional cuts");
+    if (y == nullptr && !options.reference_shape.empty())
+        throw std::invalid_argument("ambgfun reference_shape requires y");
+    const bool high_rank = options.input_shape.size() > 1 || (y != nullptr && options.reference_shape.size() > 1);
+    if (high_rank && cut != 0) throw std::invalid_argument("ambgfun high-rank input is only defined for cut='2d'");
+    const auto& ref = y == nullptr ? x : *y;
+    if (x.empty() || ref.empty()) throw std::invalid_argument("ambgfun inputs must be nonempty");
+    const int nx = detail::ambgfun_first_extent(x.size(), options.input_shape, "input");
+    const int ny = y == nullptr ? nx : detail::ambgfun_first_extent(ref.size(), options.reference_shape, "reference");
+    if (nx > std::numeric_limits<int>::max() - ny + 1)
+        throw std::invalid_argument("ambgfun input length exceeds int capacity");
+    long long count = 0;
+    int rows = 0, nfreq = 0;
+    detail::zkx_check(zkx_ambgfun_shape(nx, ny, cut, &count, &rows, &nfreq));
+    auto xs = detail::staged_c64(x);
+    DeviceArray<ComplexFloat> ys;
+    if (y != nullptr) ys = detail::staged_c64(*y);
+    DeviceArray<float> computed(static_cast<std::size_t>(count));
+    detail::zkx_check(zkx_ambgfun_c64(xs.data(), (int)x.size(), nx, y ? ys.data() : nullptr,
+                                      (int)ref.size(), ny, cut, options.fs, options.cut_value,
+                                      computed.data(), nullptr));
+    output = AmbgfunDeviceResult{};
+    const bool fp32 = cut == 0 && (std::is_same_v<T, float> || std::is_same_v<T, __half>);
+    output.dtype = fp32 ? AmbgfunOutputDtype::fp32 : AmbgfunOutputDtype::fp64;
+    output.shape = cut == 0 ? std::vector<int>{rows, nfreq} : std::vector<int>{cut == 1 ? nfreq : rows};
+    if (fp32) {
+        cuda_utils::synchronize_stream();
+        output.fp32 = std::move(computed);
+    } else {
+        output.fp64 = DeviceArray<double>(computed.size());
+        detail::zkx_check(zkx_widen_f32_to_f64(computed.data(), (long long)computed.size(),
+                                               output.fp64.data(), nullptr));
+        cuda_utils::synchronize_stream();
+    }
+}
 
 /// Matched filter of every pulse with the windowed, optionally normalised template.
 template <class T>
@@ -261,6 +353,9 @@ CaCfarDeviceResult ca_cfar_device(const DeviceArray<T>& x, const std::vector<int
 }
 
 // CPU references (declared for callers that link the reference's own CPU implementation).
+template <class T>
+AmbgfunCpuResult ambgfun_typed_cpu(const std::vector<TypedComplex<T>>& x, const AmbgfunOptions& options = {},
+                                   const std::vector<TypedComplex<T>>* y = nullptr);
 template <class T>
 CaCfarCpuResult ca_cfar_typed_cpu(const std::vector<T>& x, const std::vector<int>& shape, const CaCfarOptions& options);
 template <class T>

@@ -167,6 +167,21 @@ ZKX_API int zkx_pulse_doppler_c64(const void* x, int num_pulses, int samples_per
 ZKX_API int zkx_fft_c2c_c64(const void* x, int batch, int n, int inverse, void* y,
                             zkx_stream_t stream);
 
+/* ambgfun: normalised ambiguity function of x against y (y = NULL means y = x) and its
+ * cuts.  Replaces cusignal::ambgfun_device<float> (include/cusignal/operators/radartools/
+ * radartools_typed.h:133-137; radartools_typed.cpp:422-463, computation
+ * radartools_typed.cu:30-126).  x [x_count] complex64 of which the first nx samples enter
+ * the sums while the norm runs over all x_count (the reference's rule for high-rank
+ * inputs, whose first extent is nx); y likewise.  cut 0 = 2-D, out [nx+ny-1, nfreq];
+ * 1 = delay cut (cut_value = delay), out [nfreq]; 2 = Doppler cut (cut_value = Doppler
+ * frequency), out [nx+ny-1]; nfreq = the next power of two >= nx+ny-1, at most 65536.
+ * fs must be nonzero for the cuts.  FP32 results; a zero norm gives NaN. */
+ZKX_API int zkx_ambgfun_c64(const void* x, int x_count, int nx, const void* y, int y_count, int ny,
+                            int cut, double fs, double cut_value, float* out, zkx_stream_t stream);
+
+/* Output geometry of zkx_ambgfun_c64 (host only): element count, rows = nx+ny-1, nfreq. */
+ZKX_API int zkx_ambgfun_shape(int nx, int ny, int cut, long long* count, int* rows, int* nfreq);
+
 /* CFAR threshold multiplier alpha = N_ref * (pfa^(-1/N_ref) - 1), on the host in FP64.
  * Replaces cusignal::cfar_alpha_typed_cpu / cfar_alpha_device (radartools_typed.h:207-222,
  * radartools_typed.cpp:592-617). */

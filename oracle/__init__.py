@@ -73,6 +73,7 @@ def restatement() -> ctypes.CDLL:
         lib.or_resample_poly_design.argtypes = [_P, _D, _P]
         lib.or_resample_poly_f64.argtypes = [_P, _P, _P, _I, _I, _P]
         lib.or_resample_poly_f32.argtypes = [_P, _P, _P, _I, _I, _P]
+        lib.or_ambgfun.argtypes = [_P, _I, _I, _P, _I, _I, _I, _D, _D, _P]
         _lib_cache["r"] = lib
     return _lib_cache["r"]
 
@@ -92,6 +93,7 @@ def reference() -> Optional[ctypes.CDLL]:
         lib.zkx_ref_upfirdn_f32.argtypes = [_P, _I, _P, _I, _I, _I, _I, _P, _P]
         lib.zkx_ref_resample_poly_f32.argtypes = [_P, _I, _I, _I, _I, _D, _P, _I, _P, _P, _P]
         lib.zkx_ref_firwin_kaiser.argtypes = [_I, _D, _D, _P]
+        lib.zkx_ref_ambgfun_f32.argtypes = [_P, _I, _I, _P, _I, _I, _I, _D, _D, _P, _P]
         _lib_cache["ref"] = lib
     return _lib_cache["ref"]
 
@@ -405,3 +407,42 @@ def ref_firwin_kaiser(numtaps: int, cutoff: float, beta: float) -> np.ndarray:
     out = np.zeros(numtaps, dtype=np.float64)
     _check(lib.zkx_ref_firwin_kaiser(numtaps, cutoff, beta, out.ctypes.data), lib)
     return out
+
+
+_CUTS = {"2d": 0, "delay": 1, "doppler": 2}
+
+
+def ambgfun_shape(nx: int, ny: int, cut: str):
+    rows = nx + ny - 1
+    nfreq = 1
+    while nfreq < rows:
+        nfreq <<= 1
+    return {"2d": (rows, nfreq), "delay": (nfreq,), "doppler": (rows,)}[cut]
+
+
+def ambgfun(x, y=None, fs: float = 1.0, cut: str = "2d", cut_value: float = 0.0, nx=None, ny=None):
+    """Restatement of ambgfun_typed_cpu (rt.cpp:330-463), values in FP64.  nx / ny: the
+    first extents of high-rank inputs (default: the whole arrays)."""
+    x = _c64(x).ravel()
+    nx = x.size if nx is None else nx
+    yy = None if y is None else _c64(y).ravel()
+    ny = (nx if yy is None else yy.size) if ny is None else ny
+    shape = ambgfun_shape(nx, ny, cut)
+    out = np.empty(shape, dtype=np.float64)
+    _check(restatement().or_ambgfun(_ptr(x), x.size, nx, _ptr(yy), 0 if yy is None else yy.size, ny,
+                                    _CUTS[cut], fs, cut_value, _ptr(out)))
+    return out
+
+
+def ref_ambgfun(x, y=None, fs: float = 1.0, cut: str = "2d", cut_value: float = 0.0, nx=None, ny=None):
+    """The reference's own ambgfun_typed_cpu<float>; returns (values as float64, is_fp64)."""
+    x = _c64(x).ravel()
+    nx = x.size if nx is None else nx
+    yy = None if y is None else _c64(y).ravel()
+    ny = (nx if yy is None else yy.size) if ny is None else ny
+    out = np.empty(ambgfun_shape(nx, ny, cut), dtype=np.float64)
+    is64 = ctypes.c_int()
+    lib = reference()
+    _check(lib.zkx_ref_ambgfun_f32(_ptr(x), x.size, nx, _ptr(yy), 0 if yy is None else yy.size, ny,
+                                   _CUTS[cut], fs, cut_value, _ptr(out), ctypes.byref(is64)), lib)
+    return out, bool(is64.value)

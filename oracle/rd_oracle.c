@@ -8,6 +8,7 @@
  */
 #include "rd_oracle.h"
 
+#include <complex.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -504,5 +505,114 @@ int or_resample_poly_f32(const float* taps, const or_resample_layout* L, const f
             out[(size_t)line * L->output_samples + m] = sum;
         }
     }
+    return OR_OK;
+}
+
+/* ---------------------------------------------------------------- ambgfun */
+
+/* normalized_reference (rt.cpp:30-52): every value divided by the FP64 norm of the whole
+ * array; a zero norm gives NaN values. */
+static double complex* or_normalized(const float* v, int count)
+{
+    double sum = 0.0;
+    for (int i = 0; i < count; ++i) {
+        const double re = (double)v[2 * i], im = (double)v[2 * i + 1];
+        sum += re * re + im * im;
+    }
+    const double norm = sqrt(sum);
+    double complex* out = (double complex*)malloc(sizeof(double complex) * (size_t)(count > 0 ? count : 1));
+    for (int i = 0; i < count; ++i) {
+        if (norm == 0.0) out[i] = CMPLX(NAN, NAN);
+        else out[i] = CMPLX((double)v[2 * i] / norm, (double)v[2 * i + 1] / norm);
+    }
+    return out;
+}
+
+/* direct_transform (rt.cpp:54-72): length-point DFT of the first min(n, length) inputs,
+ * inverse with the positive exponent and 1/length. */
+static double complex* or_direct_transform(const double complex* in, int n, int length, int inverse)
+{
+    double complex* out = (double complex*)malloc(sizeof(double complex) * (size_t)length);
+    const double sign = inverse ? 1.0 : -1.0;
+    const double scale = inverse ? 1.0 / (double)length : 1.0;
+    for (int f = 0; f < length; ++f) {
+        double complex sum = 0.0;
+        for (int s = 0; s < n && s < length; ++s) {
+            const double angle = sign * 2.0 * kPi * (double)f * (double)s / (double)length;
+            sum += in[s] * CMPLX(cos(angle), sin(angle));
+        }
+        out[f] = sum * scale;
+    }
+    return out;
+}
+
+int or_ambgfun(const float* x, int x_count, int nx, const float* y, int y_count, int ny,
+               int cut, double fs, double cut_value, double* out)
+{
+    if (!y) {
+        y = x;
+        y_count = x_count;
+        ny = nx;
+    }
+    if (!x || !out || nx < 1 || ny < 1 || nx > x_count || ny > y_count || cut < 0 || cut > 2)
+        return OR_INVALID;
+    if (cut != 0 && fs == 0.0) return OR_INVALID;
+    const int rows = nx + ny - 1;
+    int nfreq = 1;
+    while (nfreq < rows) nfreq <<= 1;
+    double complex* xn = or_normalized(x, x_count);
+    double complex* yn = or_normalized(y, y_count);
+    if (cut == 0) {
+        for (int row = 0; row < rows; ++row) {
+            for (int shifted = 0; shifted < nfreq; ++shifted) {
+                const int frequency = (shifted - nfreq / 2 + nfreq) % nfreq;
+                double complex sum = 0.0;
+                for (int column = 0; column < ny; ++column) {
+                    const int xc = column - (nx - 1) + row;
+                    if (xc < 0 || xc >= nx) continue;
+                    const double angle = 2.0 * kPi * (double)frequency * (double)column / (double)nfreq;
+                    sum += yn[column] * conj(xn[xc]) * CMPLX(cos(angle), sin(angle));
+                }
+                out[(size_t)row * nfreq + shifted] = cabs(sum);
+            }
+        }
+    } else if (cut == 1) {
+        double complex* xf = or_direct_transform(xn, x_count, nfreq, 0);
+        for (int i = 0; i < nfreq; ++i) {
+            const double frequency = -fs / 2.0 + fs * (double)i / (double)nfreq;
+            const double angle = 2.0 * kPi * frequency * cut_value;
+            xf[i] *= CMPLX(cos(angle), sin(angle));
+        }
+        double complex* xs = or_direct_transform(xf, nfreq, nfreq, 1);
+        double complex* prod = (double complex*)calloc((size_t)nfreq, sizeof(double complex));
+        for (int i = 0; i < ny && i < nfreq; ++i) prod[i] = yn[i] * conj(xs[i]);
+        double complex* tr = or_direct_transform(prod, nfreq, nfreq, 1);
+        for (int i = 0; i < nfreq; ++i) out[i] = (double)nfreq * cabs(tr[(i + nfreq / 2) % nfreq]);
+        free(xf);
+        free(xs);
+        free(prod);
+        free(tr);
+    } else {
+        double complex* mod = (double complex*)malloc(sizeof(double complex) * (size_t)x_count);
+        for (int i = 0; i < x_count; ++i) mod[i] = xn[i];
+        for (int i = 0; i < nx; ++i) {
+            const double time = (double)i / fs;
+            const double angle = 2.0 * kPi * cut_value * time;
+            mod[i] *= CMPLX(cos(angle), sin(angle));
+        }
+        double complex* yf = or_direct_transform(yn, y_count, rows, 0);
+        double complex* xf = or_direct_transform(mod, x_count, rows, 0);
+        double complex* prod = (double complex*)malloc(sizeof(double complex) * (size_t)rows);
+        for (int i = 0; i < rows; ++i) prod[i] = yf[i] * conj(xf[i]);
+        double complex* tr = or_direct_transform(prod, rows, rows, 1);
+        for (int i = 0; i < rows; ++i) out[i] = cabs(tr[(i - rows / 2 + rows) % rows]);
+        free(mod);
+        free(yf);
+        free(xf);
+        free(prod);
+        free(tr);
+    }
+    free(xn);
+    free(yn);
     return OR_OK;
 }

@@ -113,6 +113,14 @@ int or_resample_poly_f64(const double* taps, const or_resample_layout* layout,
 int or_resample_poly_f32(const float* taps, const or_resample_layout* layout,
                          const float* x, int rows, int n, float* out);
 
+/* ambgfun (rt.cpp:330-463): x [x_count] complex64 of which the first nx samples enter
+ * the sums (the norm runs over all x_count); y likewise (y = NULL means y = x).
+ * cut 0 = 2-D [rows, nfreq], 1 = delay cut [nfreq], 2 = Doppler cut [rows], with
+ * rows = nx + ny - 1 and nfreq the next power of two; values in double.  Direct
+ * double-precision sums in the reference's order. */
+int or_ambgfun(const float* x, int x_count, int nx, const float* y, int y_count, int ny,
+               int cut, double fs, double cut_value, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,6 +18,7 @@
 //   resample_poly_typed_cpu      src/operators/filtering/filtering_typed.cpp:2617-2716
 //   firwin_typed_cpu             include/cusignal/operators/filter_design/filter_design_typed.h:132
 //   kaiser_typed_cpu             include/cusignal/operators/windows/windows_typed.h:169
+//   ambgfun_typed_cpu            src/operators/radartools/radartools_typed.cpp:330-463
 #include <cusignal/operators/radartools/radartools_typed.h>
 #include <cusignal/operators/filtering/filtering_typed.h>
 #include <cusignal/operators/filter_design/filter_design_typed.h>
@@ -240,3 +241,32 @@ int zkx_ref_firwin_kaiser(int numtaps, double cutoff, double beta, double* out)
 }
 
 }  // extern "C"
+
+// ambgfun_typed_cpu<float>.  x [x_count] with logical shape {nx, x_count / nx} when
+// x_count != nx (only the 2-D cut accepts that); y = NULL means y = x.  out receives the
+// values as double (FP32 results widened); *shape0 / *shape1 the result shape.
+extern "C" int zkx_ref_ambgfun_f32(const float* x, int x_count, int nx, const float* y,
+                                   int y_count, int ny, int cut, double fs, double cut_value,
+                                   double* out, int* is_fp64)
+{
+    return guarded([&] {
+        cusignal::AmbgfunOptions o;
+        o.fs = fs;
+        o.cut = static_cast<cusignal::AmbgfunCut>(cut);
+        o.cut_value = cut_value;
+        if (x_count != nx) o.input_shape = {nx, x_count / nx};
+        const auto xv = complex_vector(x, static_cast<std::size_t>(x_count));
+        std::vector<cusignal::TypedComplex<float>> yv;
+        if (y) {
+            yv = complex_vector(y, static_cast<std::size_t>(y_count));
+            if (y_count != ny) o.reference_shape = {ny, y_count / ny};
+        }
+        const auto r = cusignal::ambgfun_typed_cpu<float>(xv, o, y ? &yv : nullptr);
+        *is_fp64 = r.dtype == cusignal::AmbgfunOutputDtype::fp64 ? 1 : 0;
+        if (*is_fp64) {
+            std::memcpy(out, r.fp64.data(), r.fp64.size() * sizeof(double));
+        } else {
+            for (std::size_t i = 0; i < r.fp32.size(); ++i) out[i] = r.fp32[i];
+        }
+    });
+}

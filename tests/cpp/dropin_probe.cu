@@ -138,6 +138,32 @@ int main(int argc, char** argv)
         save("fft", spec.to_host());
         save("ifft", back.to_host());
 
+        // ambiguity function of the template, the calls Task1 step 5 makes
+        AmbgfunOptions ao;
+        ao.fs = 2.0;
+        ao.prf = 1.0;
+        AmbgfunDeviceResult a2d, adelay, adoppler;
+        ambgfun_device<float>(t, a2d, ao);
+        if (a2d.dtype != AmbgfunOutputDtype::fp32) throw std::runtime_error("2-D ambgfun of float is FP32");
+        save("amb2d", a2d.fp32.to_host());
+        ao.cut = AmbgfunCut::doppler;
+        ao.cut_value = 0.1;
+        ambgfun_device<float>(t, adoppler, ao);
+        save("ambdoppler", adoppler.fp64.to_host());
+        ao.cut = AmbgfunCut::delay;
+        ao.cut_value = 3.0;
+        ambgfun_device<float>(t, adelay, ao);
+        save("ambdelay", adelay.fp64.to_host());
+        bool amb_threw = false;
+        try {
+            ao.fs = 0.0;
+            AmbgfunDeviceResult bad;
+            ambgfun_device<float>(t, bad, ao);
+        } catch (const std::invalid_argument&) {
+            amb_threw = true;
+        }
+        if (!amb_threw) throw std::runtime_error("ambgfun with fs = 0 did not throw");
+
         // error contract: invalid shapes throw std::invalid_argument
         bool threw = false;
         try {

@@ -98,6 +98,13 @@ def test_dropin_api_matches_oracle():
         assert rel(out("resample", np.float64), O.resample_poly(s, 3, 2)) <= REL_L2
         assert rel(out("upfirdn_i16", np.float32),
                    O.upfirdn(hi.astype(np.float32), si.astype(np.float32), 2, 3)) <= REL_L2
+        a2d = out("amb2d", np.float32)
+        ref2d = O.ambgfun(t, fs=2.0, cut="2d").ravel()
+        assert np.linalg.norm(a2d - ref2d) / np.linalg.norm(ref2d) <= REL_L2
+        for name, cut, cv in (("ambdoppler", "doppler", 0.1), ("ambdelay", "delay", 3.0)):
+            got = out(name, np.float64)
+            ref = O.ambgfun(t, fs=2.0, cut=cut, cut_value=cv)
+            assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= REL_L2, name
         spec = out("fft", np.float32).view(np.complex64).reshape(P, N)
         assert rel(spec, np.fft.fft(x.astype(np.complex128), axis=1)) <= REL_L2
         assert rel(out("ifft", np.float32).view(np.complex64).reshape(P, N), x) <= 1e-6

@@ -74,6 +74,9 @@ SIGNATURES = {
     "zkx_pulse_doppler_c64": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, _P]),
     "zkx_fft_c2c_c64": (_I, [_P, _I, _I, _I, _P, _P]),
     "zkx_cfar_alpha": (_I, [_D, _I, ctypes.POINTER(_D)]),
+    "zkx_ambgfun_c64": (_I, [_P, _I, _I, _P, _I, _I, _I, _D, _D, _P, _P]),
+    "zkx_ambgfun_shape": (_I, [_I, _I, _I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I),
+                               ctypes.POINTER(_I)]),
     "zkx_cfar_reference_count": (_I, [_I, _I, _I, _I, _I]),
     "zkx_ca_cfar_f32": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _D, _I, _P, _P, _P]),
     "zkx_fir_f32": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P]),

@@ -202,6 +202,25 @@ struct FftPlan {
     static_assert((E & (E - 1)) == 0 && E >= 1 && E <= 32, "E");
 };
 
+// Values per thread for a transform of length N (a plan table chosen so that every
+// pass but the last uses the full radix and the thread count stays in 8..512).
+#ifndef ZKX_E16384
+#define ZKX_E16384 32
+#endif
+constexpr int elems_for(int n)
+{
+    return n <= 32 ? n : n == 64 ? 8 : n == 128 ? 16 : n == 256 ? 16 : n == 512 ? 32
+         : n == 1024 ? 32 : n == 2048 ? 16 : n == 4096 ? 16 : n == 8192 ? 32 : ZKX_E16384;
+}
+
+// Transforms per CTA for row kernels: aim for >= 128 threads per CTA.
+constexpr int rows_per_cta(int n)
+{
+    constexpr int kTarget = 128;
+    const int t = n / elems_for(n);
+    return t >= kTarget ? 1 : kTarget / t;
+}
+
 // Padded position of element addr of exchange buffer I (identity when PAD is false,
 // which callers use when the C interleaved transforms already spread every warp
 // access over all banks).

@@ -20,25 +20,6 @@
 namespace zkx {
 namespace {
 
-// Values per thread for a transform of length N (a plan table chosen so that every
-// pass but the last uses the full radix and the thread count stays in 8..512).
-#ifndef ZKX_E16384
-#define ZKX_E16384 32
-#endif
-constexpr int elems_for(int n)
-{
-    return n <= 32 ? n : n == 64 ? 8 : n == 128 ? 16 : n == 256 ? 16 : n == 512 ? 32
-         : n == 1024 ? 32 : n == 2048 ? 16 : n == 4096 ? 16 : n == 8192 ? 32 : ZKX_E16384;
-}
-
-// Transforms per CTA for row kernels: aim for >= 128 threads per CTA.
-constexpr int rows_per_cta(int n)
-{
-    constexpr int kTarget = 128;
-    const int t = n / elems_for(n);
-    return t >= kTarget ? 1 : kTarget / t;
-}
-
 // ------------------------------------------------------------ replica spectrum
 
 // spectrum[k] = conj(FFT(w h / ||w h||, N))[k] / N; one CTA.  The norm runs over all

@@ -47,7 +47,7 @@ int* kernel_error_word();
 // pointer stays valid until the same slot is requested with a larger size on the
 // same device.  Callers on one device must order their use of a slot on one stream.
 enum ScratchSlot { kScratchReplica = 0, kScratchDopplerWindow = 1, kScratchCfarIntegral = 2,
-                   kScratchPolyTaps = 3, kScratchSlots = 4 };
+                   kScratchPolyTaps = 3, kScratchAmbgfun = 4, kScratchSlots = 5 };
 int scratch(ScratchSlot slot, std::size_t bytes, void** out);
 
 bool is_pow2(long long n);

@@ -97,6 +97,41 @@ def fft(x: torch.Tensor, inverse: bool = False, out: Optional[torch.Tensor] = No
     return y
 
 
+_AMBGFUN_CUTS = {"2d": 0, "delay": 1, "doppler": 2}
+
+
+def ambgfun(x: torch.Tensor, fs: float, prf: float, y: Optional[torch.Tensor] = None,
+            cut: str = "2d", cutValue: float = 0.0) -> torch.Tensor:
+    """Normalised ambiguity function (cuSignal ``ambgfun(x, fs, prf, y=None, cut='2d',
+    cutValue=0)``, radartools.py).  x, y: complex64 CUDA tensors of any shape whose first
+    extent is the signal length (the norm runs over the whole tensor).  Returns float32:
+    [nx+ny-1, nfreq] for '2d', [nfreq] for 'delay', [nx+ny-1] for 'doppler'.  ``prf`` does
+    not enter the result, as in the reference."""
+    if cut not in _AMBGFUN_CUTS:
+        raise ValueError("cut must be '2d', 'delay' or 'doppler'")
+    if not isinstance(x, torch.Tensor) or not x.is_cuda or x.dtype != torch.complex64:
+        raise TypeError("x must be a complex64 CUDA tensor")
+    x = x.contiguous()
+    nx = x.shape[0] if x.ndim else 1
+    if y is not None:
+        if not y.is_cuda or y.dtype != torch.complex64:
+            raise TypeError("y must be a complex64 CUDA tensor")
+        y = y.contiguous()
+    ny = (y.shape[0] if y.ndim else 1) if y is not None else nx
+    if cut != "2d" and (x.ndim > 1 or (y is not None and y.ndim > 1)):
+        raise ValueError("ambgfun high-rank input is only defined for cut='2d'")
+    count, rows, nfreq = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int()
+    code = _AMBGFUN_CUTS[cut]
+    L.check(L.lib().zkx_ambgfun_shape(nx, ny, code, ctypes.byref(count), ctypes.byref(rows),
+                                      ctypes.byref(nfreq)))
+    shape = {0: (rows.value, nfreq.value), 1: (nfreq.value,), 2: (rows.value,)}[code]
+    out = torch.empty(shape, dtype=torch.float32, device=x.device)
+    L.check(L.lib().zkx_ambgfun_c64(x.data_ptr(), x.numel(), nx, L.ptr(y),
+                                    0 if y is None else y.numel(), ny, code, float(fs),
+                                    float(cutValue), out.data_ptr(), L.stream_handle()))
+    return out
+
+
 def pulse_doppler(x: torch.Tensor, window: WindowArg = None, nfft: Optional[int] = None,
                   return_power: bool = False):
     """FFT along pulses (axis 0) of window[p] * x[p, n]; returns complex64 [nfft, N]
