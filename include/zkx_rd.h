@@ -182,6 +182,40 @@ ZKX_API int zkx_ambgfun_c64(const void* x, int x_count, int nx, const void* y, i
 /* Output geometry of zkx_ambgfun_c64 (host only): element count, rows = nx+ny-1, nfreq. */
 ZKX_API int zkx_ambgfun_shape(int nx, int ny, int cut, long long* count, int* rows, int* nfreq);
 
+/* ---------------------------------------------------------------- synthesis
+ * Inputs generated on the device (no counterpart entry in the reference library; the
+ * Task1 pair replaces the kernels of ZKX/Task1/pipeline/src/steps/step1/step1.cu:11-71). */
+
+/* Task1 LFM waveform: out[i] = exp(i pi (B / T) t^2), t = i / fs - T / 2, T = length / fs
+ * (phase in FP64). */
+ZKX_API int zkx_lfm_waveform_c64(int length, double sample_rate, double bandwidth, void* out,
+                                 zkx_stream_t stream);
+
+/* Task1 echo [num_pulses, samples_per_pulse]: the waveform delayed by `delay` samples with
+ * Doppler phase exp(2 pi i f_d (p / prf + n / fs)) times amplitude (noiseless), uniform
+ * noise in [-noise_std, noise_std] from the reference's per-element hash of `seed`
+ * (bit-identical), and their sum (echo).  Any of the three outputs may be NULL. */
+ZKX_API int zkx_task1_echo_c64(const void* waveform, int pulse_samples, int num_pulses,
+                               int samples_per_pulse, int delay, double doppler_hz, uint32_t seed,
+                               double prf, double sample_rate, double amplitude, double noise_std,
+                               void* noiseless, void* noise, void* echo, zkx_stream_t stream);
+
+/* One point target of the synthetic CPI model. */
+typedef struct {
+    int delay;         /* range delay in samples */
+    int doppler_bin;   /* Doppler ramp exp(2 pi i bin p / num_pulses) */
+    double amplitude;
+    double phase;      /* radians */
+} zkx_synth_target;
+
+/* Synthetic CPI [num_pulses, samples_per_pulse]: CN(0, noise_power) noise from a
+ * counter-based generator keyed by `seed` (a pure function of seed and element index)
+ * plus up to 64 targets, each amplitude * s[n - delay] * exp(i (2 pi bin p / P + phase))
+ * with the chirp s[m] = exp(i pi (bandwidth / L) (m - L/2)^2), m < chirp_length. */
+ZKX_API int zkx_synth_cpi_c64(int num_pulses, int samples_per_pulse, int chirp_length,
+                              double bandwidth, const zkx_synth_target* targets, int n_targets,
+                              uint64_t seed, double noise_power, void* out, zkx_stream_t stream);
+
 /* CFAR threshold multiplier alpha = N_ref * (pfa^(-1/N_ref) - 1), on the host in FP64.
  * Replaces cusignal::cfar_alpha_typed_cpu / cfar_alpha_device (radartools_typed.h:207-222,
  * radartools_typed.cpp:592-617). */

@@ -74,6 +74,8 @@ def restatement() -> ctypes.CDLL:
         lib.or_resample_poly_f64.argtypes = [_P, _P, _P, _I, _I, _P]
         lib.or_resample_poly_f32.argtypes = [_P, _P, _P, _I, _I, _P]
         lib.or_ambgfun.argtypes = [_P, _I, _I, _P, _I, _I, _I, _D, _D, _P]
+        lib.or_task1_echo.argtypes = [_P, _I, _I, _I, _I, _D, ctypes.c_uint32, _D, _D, _D,
+                                      ctypes.c_float, _P, _P]
         _lib_cache["r"] = lib
     return _lib_cache["r"]
 
@@ -446,3 +448,15 @@ def ref_ambgfun(x, y=None, fs: float = 1.0, cut: str = "2d", cut_value: float = 
     _check(lib.zkx_ref_ambgfun_f32(_ptr(x), x.size, nx, _ptr(yy), 0 if yy is None else yy.size, ny,
                                    _CUTS[cut], fs, cut_value, _ptr(out), ctypes.byref(is64)), lib)
     return out, bool(is64.value)
+
+
+def task1_echo(waveform, pulses: int, samples: int, delay: int, doppler_hz: float, seed: int,
+               prf: float, fs: float, amplitude: float, noise_std: float):
+    """Task1 step-1 echo (step1.cu:11-71): (noiseless complex128 [P, N] with FP64 phases,
+    noise complex64 [P, N] bit-exact to the reference's hash)."""
+    w = _c64(waveform)
+    noiseless = np.empty((pulses, samples), dtype=np.complex128)
+    noise = np.empty((pulses, samples), dtype=np.complex64)
+    _check(restatement().or_task1_echo(_ptr(w), w.size, pulses, samples, delay, doppler_hz, seed, prf, fs,
+                                       amplitude, noise_std, _ptr(noiseless), _ptr(noise)))
+    return noiseless, noise

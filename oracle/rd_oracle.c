@@ -616,3 +616,45 @@ int or_ambgfun(const float* x, int x_count, int nx, const float* y, int y_count,
     free(yn);
     return OR_OK;
 }
+
+/* ------------------------------------------------------------ Task1 echo */
+
+static uint32_t or_task1_hash(uint32_t index, uint32_t seed)
+{
+    uint32_t v = seed ^ (index * 747796405U + 2891336453U);
+    v ^= v >> 16;
+    v *= 2246822519U;
+    v ^= v >> 13;
+    v *= 3266489917U;
+    return v ^ (v >> 16);
+}
+
+int or_task1_echo(const float* waveform, int L, int P, int N, int delay, double fd, uint32_t seed,
+                  double prf, double fs, double amplitude, float noise_std, double* noiseless,
+                  float* noise)
+{
+    if (!waveform || P < 1 || N < 1 || L < 1 || delay < 0 || delay + L > N) return OR_INVALID;
+    for (long long e = 0; e < (long long)P * N; ++e) {
+        const int p = (int)(e / N), n = (int)(e % N);
+        double re = 0.0, im = 0.0;
+        const int src = n - delay;
+        if (src >= 0 && src < L) {
+            const double t = (double)p / prf + (double)n / fs;
+            const double ph = 2.0 * kPi * fd * t;
+            const double c = cos(ph), s = sin(ph);
+            const double wr = waveform[2 * src], wi = waveform[2 * src + 1];
+            re = amplitude * (wr * c - wi * s);
+            im = amplitude * (wr * s + wi * c);
+        }
+        if (noiseless) {
+            noiseless[2 * e] = re;
+            noiseless[2 * e + 1] = im;
+        }
+        if (noise) {
+            const uint32_t k = (uint32_t)(2 * e);
+            noise[2 * e] = ((float)(or_task1_hash(k, seed) & 0xffffU) / 32767.5F - 1.0F) * noise_std;
+            noise[2 * e + 1] = ((float)(or_task1_hash(k + 1U, seed) & 0xffffU) / 32767.5F - 1.0F) * noise_std;
+        }
+    }
+    return OR_OK;
+}

@@ -121,6 +121,13 @@ int or_resample_poly_f32(const float* taps, const or_resample_layout* layout,
 int or_ambgfun(const float* x, int x_count, int nx, const float* y, int y_count, int ny,
                int cut, double fs, double cut_value, double* out);
 
+/* Task1 step 1 echo (ZKX/Task1/pipeline/src/steps/step1/step1.cu:11-71): uniform noise
+ * from the reference's per-element hash (exact FP32), target = amplitude * waveform delayed
+ * with the Doppler phase in FP64.  noise, noiseless: [P * N] complex (float / double). */
+int or_task1_echo(const float* waveform, int pulse_samples, int num_pulses, int samples_per_pulse,
+                  int delay, double doppler_hz, uint32_t seed, double prf, double sample_rate,
+                  double amplitude, float noise_std, double* noiseless, float* noise);
+
 #ifdef __cplusplus
 }
 #endif

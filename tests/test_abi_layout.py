@@ -20,6 +20,7 @@ STRUCTS = {
     "zkx_rd_server_desc": L.ServerDesc,
     "zkx_rd_request": L.Request,
     "zkx_rd_server_stats": L.ServerStats,
+    "zkx_synth_target": L.SynthTarget,
 }
 
 

@@ -62,6 +62,10 @@ class ServerStats(ctypes.Structure):
                 ("peak_bytes", ctypes.c_size_t), ("plan_bytes", ctypes.c_size_t), ("plans", _I)]
 
 
+class SynthTarget(ctypes.Structure):
+    _fields_ = [("delay", _I), ("doppler_bin", _I), ("amplitude", _D), ("phase", _D)]
+
+
 SIGNATURES = {
     "zkx_last_error": (ctypes.c_char_p, []),
     "zkx_version": (ctypes.c_char_p, []),
@@ -75,6 +79,9 @@ SIGNATURES = {
     "zkx_fft_c2c_c64": (_I, [_P, _I, _I, _I, _P, _P]),
     "zkx_cfar_alpha": (_I, [_D, _I, ctypes.POINTER(_D)]),
     "zkx_ambgfun_c64": (_I, [_P, _I, _I, _P, _I, _I, _I, _D, _D, _P, _P]),
+    "zkx_lfm_waveform_c64": (_I, [_I, _D, _D, _P, _P]),
+    "zkx_task1_echo_c64": (_I, [_P, _I, _I, _I, _I, _D, ctypes.c_uint32, _D, _D, _D, _D, _P, _P, _P, _P]),
+    "zkx_synth_cpi_c64": (_I, [_I, _I, _I, _D, ctypes.POINTER(SynthTarget), _I, ctypes.c_uint64, _D, _P, _P]),
     "zkx_ambgfun_shape": (_I, [_I, _I, _I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I),
                                ctypes.POINTER(_I)]),
     "zkx_cfar_reference_count": (_I, [_I, _I, _I, _I, _I]),

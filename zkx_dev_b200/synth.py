@@ -90,3 +90,62 @@ def firwin_kaiser(numtaps: int, cutoff: float, beta: float) -> np.ndarray:
     w = i0(beta * np.sqrt(np.clip(1.0 - (m / alpha) ** 2, 0.0, None))) / i0(beta)
     h = h * w
     return h / h.sum()
+
+
+# ------------------------------------------------------------ device generation
+
+def draw_targets(pulses: int, samples: int, n_targets: int, chirp_length: int, seed: int,
+                 snr_db: Tuple[float, float] = (10.0, 30.0)) -> List[Target]:
+    """Seeded targets of the CPI model (delay, Doppler bin, SNR, phase) for device_cpi."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_targets):
+        delay = int(rng.integers(0, max(1, samples - chirp_length + 1)))
+        dop = int(rng.integers(0, pulses))
+        snr = float(rng.uniform(*snr_db))
+        out.append(Target(delay, dop, snr, float(rng.uniform(0.0, 2.0 * np.pi))))
+    return out
+
+
+def device_cpi(pulses: int, samples: int, targets: List[Target], chirp_length: int, seed: int,
+               noise_power: float = 1.0, bandwidth: float = 0.5, out=None, stream=None):
+    """The CPI model generated on the current CUDA device (zkx_synth_cpi_c64): CN(0,
+    noise_power) noise that is a pure function of (seed, element) plus the targets, each
+    amplitude 10^(snr/20) times the chirp of lfm_chirp(chirp_length, bandwidth).  Returns a
+    complex64 CUDA tensor [pulses, samples]; nothing crosses PCIe but the target table."""
+    import torch
+    from . import _lib as L
+    if len(targets) > 64:
+        raise ValueError("at most 64 targets")
+    table = (L.SynthTarget * max(1, len(targets)))()
+    for i, t in enumerate(targets):
+        table[i] = L.SynthTarget(t.delay, t.doppler_bin, 10.0 ** (t.snr_db / 20.0), t.phase)
+    if out is None:
+        out = torch.empty((pulses, samples), dtype=torch.complex64, device="cuda")
+    L.check(L.lib().zkx_synth_cpi_c64(pulses, samples, chirp_length, bandwidth, table, len(targets),
+                                      seed & 0xFFFFFFFFFFFFFFFF, noise_power, out.data_ptr(),
+                                      L.stream_handle(stream)))
+    return out
+
+
+def device_lfm(length: int, sample_rate: float, bandwidth: float):
+    """Task1 LFM waveform on the device (zkx_lfm_waveform_c64), complex64 [length]."""
+    import torch
+    from . import _lib as L
+    out = torch.empty(length, dtype=torch.complex64, device="cuda")
+    L.check(L.lib().zkx_lfm_waveform_c64(length, sample_rate, bandwidth, out.data_ptr(), L.stream_handle()))
+    return out
+
+
+def device_task1_echo(waveform, pulses: int, samples: int, delay: int, doppler_hz: float, seed: int,
+                      prf: float, sample_rate: float, amplitude: float, noise_std: float):
+    """Task1 step-1 echo on the device (zkx_task1_echo_c64): (noiseless, noise, echo),
+    complex64 CUDA tensors [pulses, samples]."""
+    import torch
+    from . import _lib as L
+    outs = [torch.empty((pulses, samples), dtype=torch.complex64, device="cuda") for _ in range(3)]
+    L.check(L.lib().zkx_task1_echo_c64(waveform.data_ptr(), waveform.numel(), pulses, samples, delay,
+                                       doppler_hz, seed & 0xFFFFFFFF, prf, sample_rate, amplitude, noise_std,
+                                       outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(),
+                                       L.stream_handle()))
+    return tuple(outs)
