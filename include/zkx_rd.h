@@ -358,6 +358,28 @@ ZKX_API int zkx_rd_execute_batch(zkx_rd_plan plan, const void* x, int batch, voi
                                  void* rd, float* power, float* threshold, uint8_t* detections,
                                  zkx_stream_t stream);
 
+/* ---------------------------------------------------------------- autotuning
+ * Per-shape kernel choices of a plan (no counterpart in the reference).  0 in a field
+ * means the library's shape heuristic. */
+enum {
+    ZKX_COMPRESSION_DEFAULT = 0,
+    ZKX_COMPRESSION_PLAIN = 1,       /* one launch per group of pulses */
+    ZKX_COMPRESSION_PERSISTENT = 2   /* persistent CTAs prefetching the next pulse (N >= 4096) */
+};
+typedef struct {
+    int compression_variant;  /* ZKX_COMPRESSION_* */
+    int doppler_columns;      /* range columns per CTA of the bulk-copy Doppler kernel: 8 or 16 */
+} zkx_rd_tuning;
+
+/* Times every candidate of each stage on `batch` CPIs at x (device, the plan's shape) on
+ * `stream`, keeps the fastest in the plan and in a process-wide table keyed by the plan's
+ * shape, which plans created later with that shape start from.  Synchronises the stream;
+ * allocates and frees temporary device buffers; run it at set-up, not in a timed loop. */
+ZKX_API int zkx_rd_plan_autotune(zkx_rd_plan plan, const void* x, int batch, zkx_stream_t stream,
+                                 zkx_rd_tuning* chosen);
+ZKX_API int zkx_rd_plan_get_tuning(zkx_rd_plan plan, zkx_rd_tuning* tuning);
+ZKX_API int zkx_rd_plan_set_tuning(zkx_rd_plan plan, const zkx_rd_tuning* tuning);
+
 /* A CUDA graph of one zkx_rd_execute_batch with fixed pointers: create runs the chain once
  * eagerly (allocating any plan-owned buffer), then captures and instantiates it; launch
  * replays it on `stream` with one call.  No counterpart in the reference. */

@@ -21,6 +21,7 @@ STRUCTS = {
     "zkx_rd_request": L.Request,
     "zkx_rd_server_stats": L.ServerStats,
     "zkx_synth_target": L.SynthTarget,
+    "zkx_rd_tuning": L.RdTuning,
 }
 
 

@@ -41,6 +41,10 @@ class RdDesc(ctypes.Structure):
                 ("reference_cells", _I * 2), ("pfa", _D), ("cfar_mode", _I), ("precision", _I)]
 
 
+class RdTuning(ctypes.Structure):
+    _fields_ = [("compression_variant", _I), ("doppler_columns", _I)]
+
+
 class ServerDesc(ctypes.Structure):
     _fields_ = [("normalize", _I), ("range_window", _I), ("doppler_window", _I),
                 ("guard_cells", _I * 2), ("reference_cells", _I * 2), ("pfa", _D),
@@ -105,6 +109,9 @@ SIGNATURES = {
     "zkx_rd_graph_create": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, ctypes.POINTER(_P)]),
     "zkx_rd_graph_launch": (_I, [_P, _P]),
     "zkx_rd_graph_destroy": (_I, [_P]),
+    "zkx_rd_plan_autotune": (_I, [_P, _P, _I, _P, ctypes.POINTER(RdTuning)]),
+    "zkx_rd_plan_get_tuning": (_I, [_P, ctypes.POINTER(RdTuning)]),
+    "zkx_rd_plan_set_tuning": (_I, [_P, ctypes.POINTER(RdTuning)]),
     "zkx_rd_server_create": (_I, [ctypes.POINTER(ServerDesc), ctypes.POINTER(_P)]),
     "zkx_rd_server_destroy": (_I, [_P]),
     "zkx_rd_submit": (_I, [_P, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]),

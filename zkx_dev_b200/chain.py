@@ -124,6 +124,22 @@ class RangeDopplerChain:
                                             ctypes.byref(g)))
         return ChainGraph(g, (x, out, self))
 
+    def autotune(self, x: torch.Tensor) -> Dict[str, int]:
+        """Time the kernel candidates of each stage on x ([P, N] or [B, P, N]) and keep the
+        fastest for this plan and for later plans of the same shape (zkx_rd_plan_autotune)."""
+        x = x.contiguous()
+        batch = x.shape[0] if x.ndim == 3 else 1
+        t = L.RdTuning()
+        L.check(L.lib().zkx_rd_plan_autotune(self._plan, x.data_ptr(), batch, L.stream_handle(),
+                                             ctypes.byref(t)))
+        return {"compression_variant": t.compression_variant, "doppler_columns": t.doppler_columns}
+
+    @property
+    def tuning(self) -> Dict[str, int]:
+        t = L.RdTuning()
+        L.check(L.lib().zkx_rd_plan_get_tuning(self._plan, ctypes.byref(t)))
+        return {"compression_variant": t.compression_variant, "doppler_columns": t.doppler_columns}
+
     def close(self) -> None:
         if getattr(self, "_plan", None) is not None and self._plan.value:
             L.lib().zkx_rd_plan_destroy(self._plan)

@@ -3,7 +3,11 @@
 #include "fft_core.cuh"
 #include "zkx_internal.h"
 
+#include <algorithm>
 #include <climits>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cmath>
 #include <numeric>
 #include <string>
@@ -162,7 +166,7 @@ extern "C" int zkx_pulse_doppler_c64(const void* x, int P, int N, int nfft, int 
         ZKX_TRY(launch_doppler_window(P, kind, w, win, stream));
     }
     return launch_pulse_doppler(static_cast<const float2*>(x), P, N, nfft, win,
-                                static_cast<float2*>(out), power, 1, stream);
+                                static_cast<float2*>(out), power, 1, 0, stream);
 }
 
 extern "C" int zkx_fft_c2c_c64(const void* x, int batch, int n, int inverse, void* y,
@@ -385,7 +389,22 @@ struct zkx_rd_plan_s {
     float* cumulative = nullptr;   // compat CFAR integral image
     size_t cumulative_elems = 0;
     CfarGeometry cfar;
+    zkx_rd_tuning tuning{};        // per-shape kernel choices (0 = heuristic)
 };
+
+namespace {
+// Autotuned kernel choices per plan shape, shared by every plan of the process.
+struct TuneKey {
+    int pulses, samples, range_nfft, doppler_nfft;
+    bool operator<(const TuneKey& o) const
+    {
+        return std::tie(pulses, samples, range_nfft, doppler_nfft) <
+               std::tie(o.pulses, o.samples, o.range_nfft, o.doppler_nfft);
+    }
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, zkx_rd_tuning> g_tune_table;
+}  // namespace
 
 namespace {
 void release_plan(zkx_rd_plan p)
@@ -452,6 +471,11 @@ extern "C" int zkx_rd_plan_create(const zkx_rd_desc* d, const void* replica,
         release_plan(p);
         return rc;
     }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        auto it = g_tune_table.find(TuneKey{P, N, nr, nd});
+        if (it != g_tune_table.end()) p->tuning = it->second;
+    }
     *out = p;
     return ZKX_SUCCESS;
 }
@@ -517,10 +541,11 @@ int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compresse
                                                N, nr, p->spectrum, static_cast<float2*>(compressed),
                                                stream));
     else
-        ZKX_TRY(launch_pulse_compression(static_cast<const float2*>(x), batch * P, N, nr, p->spectrum,
-                                         static_cast<float2*>(compressed), stream));
-    ZKX_TRY(launch_pulse_doppler(static_cast<const float2*>(compressed), P, nr, nd,
-                                 p->doppler_window, static_cast<float2*>(rd), power, batch, stream));
+        ZKX_TRY(launch_pulse_compression_variant(static_cast<const float2*>(x), batch * P, N, nr, p->spectrum,
+                                                 static_cast<float2*>(compressed),
+                                                 p->tuning.compression_variant, stream));
+    ZKX_TRY(launch_pulse_doppler(static_cast<const float2*>(compressed), P, nr, nd, p->doppler_window,
+                                 static_cast<float2*>(rd), power, batch, p->tuning.doppler_columns, stream));
     const int* gd = p->d.guard_cells;
     const int* rf = p->d.reference_cells;
     if (p->d.cfar_mode == ZKX_CFAR_COMPAT) {
@@ -549,6 +574,116 @@ extern "C" int zkx_rd_execute(zkx_rd_plan p, const void* x, void* compressed, vo
                               zkx_stream_t stream)
 {
     return zkx_rd_execute_batch(p, x, 1, compressed, rd, power, threshold, detections, stream);
+}
+
+// ------------------------------------------------------------ autotuning
+
+namespace {
+// Median time in ms of `reps` launches of f on stream s after two warm-ups.
+template <class F>
+int time_median(F&& f, cudaStream_t s, float* ms)
+{
+    constexpr int kReps = 5;
+    cudaEvent_t a, b;
+    ZKX_CUDA(cudaEventCreate(&a));
+    cudaError_t e = cudaEventCreate(&b);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(a);
+        return cuda_status(e, "autotune event");
+    }
+    float t[kReps];
+    int rc = ZKX_SUCCESS;
+    for (int i = 0; i < 2 && rc == ZKX_SUCCESS; ++i) rc = f();
+    for (int i = 0; i < kReps && rc == ZKX_SUCCESS; ++i) {
+        cudaEventRecord(a, s);
+        rc = f();
+        cudaEventRecord(b, s);
+        e = cudaEventSynchronize(b);
+        if (rc == ZKX_SUCCESS && e != cudaSuccess) rc = cuda_status(e, "autotune timing");
+        if (rc == ZKX_SUCCESS) cudaEventElapsedTime(&t[i], a, b);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc != ZKX_SUCCESS) return rc;
+    std::sort(t, t + kReps);
+    *ms = t[kReps / 2];
+    return ZKX_SUCCESS;
+}
+}  // namespace
+
+extern "C" int zkx_rd_plan_autotune(zkx_rd_plan p, const void* x, int batch, zkx_stream_t stream,
+                                    zkx_rd_tuning* chosen)
+{
+    if (!p || !x) return fail(ZKX_INVALID_ARGUMENT, "rd_plan_autotune: null pointer");
+    if (batch < 1) return fail(ZKX_INVALID_SHAPE, "rd_plan_autotune: batch must be positive");
+    const int P = p->d.num_pulses, N = p->d.samples_per_pulse, nr = p->range_nfft, nd = p->doppler_nfft;
+    const size_t cube = (size_t)batch * P * nr, map = (size_t)batch * nd * nr;
+    float2* comp = nullptr;
+    float* power = nullptr;
+    ZKX_CUDA(cudaMalloc(&comp, cube * sizeof(float2)));
+    cudaError_t e = cudaMalloc(&power, map * sizeof(float));
+    if (e != cudaSuccess) {
+        cudaFree(comp);
+        return cuda_status(e, "rd_plan_autotune allocation");
+    }
+    zkx_rd_tuning best = p->tuning;
+    int rc = ZKX_SUCCESS;
+    if (p->d.precision == ZKX_PRECISION_FP32) {
+        float tbest = 0.f;
+        for (int v : {ZKX_COMPRESSION_PLAIN, ZKX_COMPRESSION_PERSISTENT}) {
+            float ms = 0.f;
+            rc = time_median([&] {
+                return launch_pulse_compression_variant(static_cast<const float2*>(x), batch * P, N, nr,
+                                                        p->spectrum, comp, v, stream);
+            }, stream, &ms);
+            if (rc != ZKX_SUCCESS) break;
+            if (v == ZKX_COMPRESSION_PLAIN || ms < tbest) {
+                tbest = ms;
+                best.compression_variant = v;
+            }
+        }
+    }
+    if (rc == ZKX_SUCCESS) {
+        float tbest = 0.f;
+        for (int c : {16, 8}) {
+            float ms = 0.f;
+            rc = time_median([&] {
+                return launch_pulse_doppler(comp, P, nr, nd, p->doppler_window, nullptr, power, batch, c, stream);
+            }, stream, &ms);
+            if (rc != ZKX_SUCCESS) break;
+            if (c == 16 || ms < tbest) {
+                tbest = ms;
+                best.doppler_columns = c;
+            }
+        }
+    }
+    cudaFree(comp);
+    cudaFree(power);
+    if (rc != ZKX_SUCCESS) return rc;
+    p->tuning = best;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        g_tune_table[TuneKey{P, N, nr, nd}] = best;
+    }
+    if (chosen) *chosen = best;
+    return ZKX_SUCCESS;
+}
+
+extern "C" int zkx_rd_plan_get_tuning(zkx_rd_plan p, zkx_rd_tuning* t)
+{
+    if (!p || !t) return fail(ZKX_INVALID_ARGUMENT, "rd_plan_get_tuning: null pointer");
+    *t = p->tuning;
+    return ZKX_SUCCESS;
+}
+
+extern "C" int zkx_rd_plan_set_tuning(zkx_rd_plan p, const zkx_rd_tuning* t)
+{
+    if (!p || !t) return fail(ZKX_INVALID_ARGUMENT, "rd_plan_set_tuning: null pointer");
+    if (t->compression_variant < 0 || t->compression_variant > 2 ||
+        (t->doppler_columns != 0 && t->doppler_columns != 8 && t->doppler_columns != 16))
+        return fail(ZKX_INVALID_ARGUMENT, "rd_plan_set_tuning: unknown kernel choice");
+    p->tuning = *t;
+    return ZKX_SUCCESS;
 }
 
 // ------------------------------------------------------------ graph capture

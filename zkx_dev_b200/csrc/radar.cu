@@ -274,17 +274,18 @@ pulse_doppler_kernel(const float2* __restrict__ x, int pulses, int samples,
 // bandwidth this way than with per-thread loads, whose throughput is bounded by the
 // requests a thread can keep in flight.  The tile buffer doubles as the exchange
 // buffer once every thread has read its values.
-template <int N>
-__global__ void __launch_bounds__(16 * FftPlan<N, elems_for(N)>::T)
+template <int N, int C>
+__global__ void __launch_bounds__(C * FftPlan<N, elems_for(N)>::T)
 pulse_doppler_tma_kernel(const __grid_constant__ CUtensorMap tmap, int pulses, int samples,
                          const float* __restrict__ window, float2* __restrict__ out,
                          float* __restrict__ power, const float2* __restrict__ tw, int* err)
 {
     using PL = FftPlan<N, elems_for(N)>;
-    constexpr int C = 16;
     constexpr int BOXH = N < 256 ? N : 256;
     extern __shared__ __align__(128) float2 sm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + N * C);
+    // the exchange of a narrower tile is padded and can outgrow the landed tile
+    constexpr int SPAN = C < 16 && C * PL::smem_elems(true) > N * C ? C * PL::smem_elems(true) : N * C;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + SPAN);
     const int c = threadIdx.x % C;
     const int t = threadIdx.x / C;
     const int col0 = blockIdx.x * C;
@@ -320,7 +321,7 @@ pulse_doppler_tma_kernel(const __grid_constant__ CUtensorMap tmap, int pulses, i
         v[r] = a;
     }
     __syncthreads();
-    fft_block<PL, -1, C, false>(v, sm + c, t, tw);
+    fft_block<PL, -1, C, (C < 16)>(v, sm + c, t, tw);
     if (active) {
 #pragma unroll
         for (int r = 0; r < PL::E; ++r) {
@@ -356,13 +357,14 @@ int replica_impl(const float2* h, int length, int normalize, int kind, const flo
 
 template <int N, class Src>
 int compression_impl(const Src& x, bool aligned16, int pulses, int samples, const float2* spectrum,
-                     float2* y, cudaStream_t s)
+                     float2* y, int variant, cudaStream_t s)
 {
     if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
     using PL = FftPlan<N, elems_for(N)>;
     if constexpr (N >= 4096) {
-        // persistent bulk-copy pipeline: 16-byte aligned pulses (even length, aligned bases)
-        if (aligned16) {
+        // persistent bulk-copy pipeline: 16-byte aligned pulses (even length, aligned bases);
+        // variant ZKX_COMPRESSION_PLAIN keeps the one-launch-per-pulse-group kernel
+        if (aligned16 && variant != ZKX_COMPRESSION_PLAIN) {
             int dev = 0, sms = 0;
             ZKX_CUDA(cudaGetDevice(&dev));
             ZKX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -388,9 +390,25 @@ int compression_impl(const Src& x, bool aligned16, int pulses, int samples, cons
     return ZKX_SUCCESS;
 }
 
+template <int N, int CT>
+int doppler_tma(const CUtensorMap& map, int pulses, int samples, const float* window, float2* out,
+                float* power, int batch, cudaStream_t s)
+{
+    using PL = FftPlan<N, elems_for(N)>;
+    constexpr int SPAN = CT < 16 && CT * PL::smem_elems(true) > N * CT ? CT * PL::smem_elems(true) : N * CT;
+    const size_t smem = (size_t)SPAN * sizeof(float2) + 16;
+    auto k = pulse_doppler_tma_kernel<N, CT>;
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const dim3 tiles((samples + CT - 1) / CT, batch);
+    k<<<tiles, CT * PL::T, smem, s>>>(map, pulses, samples, window, out, power, twiddle_table(),
+                                      kernel_error_word());
+    ZKX_LAUNCHED("pulse_doppler_tma_kernel");
+    return ZKX_SUCCESS;
+}
+
 template <int N>
 int doppler_impl(const float2* x, int pulses, int samples, const float* window, float2* out,
-                 float* power, int batch, cudaStream_t s)
+                 float* power, int batch, int columns, cudaStream_t s)
 {
     if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
     using PL = FftPlan<N, elems_for(N)>;
@@ -402,16 +420,14 @@ int doppler_impl(const float2* x, int pulses, int samples, const float* window, 
         if ((samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
             CUtensorMap map;
             constexpr int BOXH = N < 256 ? N : 256;
+            // columns per CTA on the bulk-copy path: 8 (two tiles of 64 KB per SM overlap
+            // each other's copy, transform and stores) measured faster from 512 pulses up,
+            // 16 below; `columns` overrides (the autotuner's choice)
+            const int ct = columns == 8 || columns == 16 ? columns : (N >= 512 ? 8 : 16);
             if (encode_tensor_map_2d_f32(&map, x, 2ull * samples, (uint64_t)pulses * batch,
-                                         (uint64_t)samples * sizeof(float2), 32, BOXH)) {
-                const size_t smem = (size_t)N * C * sizeof(float2) + 16;
-                auto k = pulse_doppler_tma_kernel<N>;
-                ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                k<<<blocks, C * PL::T, smem, s>>>(map, pulses, samples, window, out, power,
-                                                  twiddle_table(), kernel_error_word());
-                ZKX_LAUNCHED("pulse_doppler_tma_kernel");
-                return ZKX_SUCCESS;
-            }
+                                         (uint64_t)samples * sizeof(float2), 2 * ct, BOXH))
+                return ct == 8 ? doppler_tma<N, 8>(map, pulses, samples, window, out, power, batch, s)
+                               : doppler_tma<N, 16>(map, pulses, samples, window, out, power, batch, s);
         }
     }
     const size_t smem = (size_t)C * PL::smem_elems(C < 16) * sizeof(float2);
@@ -472,11 +488,18 @@ int launch_replica_spectrum(const float2* replica, int length, int nfft, int nor
 int launch_pulse_compression(const float2* x, int pulses, int samples, int nfft,
                              const float2* spectrum, float2* y, cudaStream_t stream)
 {
+    return launch_pulse_compression_variant(x, pulses, samples, nfft, spectrum, y, ZKX_COMPRESSION_DEFAULT,
+                                            stream);
+}
+
+int launch_pulse_compression_variant(const float2* x, int pulses, int samples, int nfft,
+                                     const float2* spectrum, float2* y, int variant, cudaStream_t stream)
+{
     const RowsContiguous src{x, samples};
     if (nfft > (1 << kMaxSmemFftLog))
         return launch_long_compression(src, pulses, samples, nfft, spectrum, y, stream);
     const bool aligned16 = (samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0;
-#define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, stream)
+#define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, variant, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
 #undef ZKX_CALL
 }
@@ -498,16 +521,16 @@ int launch_pulse_compression_table(const float2* const* cpis, int count, int pul
     const int pulses = count * pulses_per_cpi;
     if (nfft > (1 << kMaxSmemFftLog))
         return launch_long_compression(src, pulses, samples, nfft, spectrum, y, stream);
-#define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, stream)
+#define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, ZKX_COMPRESSION_DEFAULT, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
 #undef ZKX_CALL
 }
 
 int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft, const float* window,
-                         float2* out, float* power, int batch, cudaStream_t stream)
+                         float2* out, float* power, int batch, int columns, cudaStream_t stream)
 {
     if (nfft > 4096) return fail(ZKX_UNSUPPORTED_OPERATION, "pulse_doppler: nfft above 4096 is not supported");
-#define ZKX_CALL(NN) doppler_impl<NN>(x, pulses, samples, window, out, power, batch, stream)
+#define ZKX_CALL(NN) doppler_impl<NN>(x, pulses, samples, window, out, power, batch, columns, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
 #undef ZKX_CALL
 }

@@ -63,8 +63,13 @@ int launch_pulse_compression(const float2* x, int pulses, int samples, int nfft,
 int launch_pulse_compression_tc(const float2* x, int pulses, int samples, int nfft,
                                 const float2* spectrum, float2* y, int precision,
                                 cudaStream_t stream);
+// Compression kernel choice: the library's default, the one-launch-per-pulse-group kernel,
+// or the persistent bulk-copy pipeline (N >= 4096, 16-byte aligned pulses).
+int launch_pulse_compression_variant(const float2* x, int pulses, int samples, int nfft,
+                                     const float2* spectrum, float2* y, int variant, cudaStream_t stream);
+// columns: range columns per CTA of the bulk-copy Doppler kernel (8 or 16; 0 = by shape).
 int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft,
-                         const float* window, float2* out, float* power, int batch,
+                         const float* window, float2* out, float* power, int batch, int columns,
                          cudaStream_t stream);
 int launch_fft_rows(const float2* x, int rows, int n, int inverse, float2* y, cudaStream_t stream);
 // Lengths 32768 and 65536 (thread-block clusters, long_fft.cu); the spectrum of a long
