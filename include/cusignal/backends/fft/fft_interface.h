@@ -1,8 +1,9 @@
 // Complex types and the batched device FFT of the cusignal_cpp FFT backend
 // (ZKX/cusignal_cpp/include/cusignal/backends/fft/fft_interface.h:104-117, 499-536):
 // forward transforms are unnormalised, inverse transforms scale by 1/N.  Lengths are
-// powers of two up to 65536; the device calls run the B200 shared-memory FFT on the
-// legacy default stream.
+// powers of two up to 65536 and any other length up to 32768 (chirp-z on power-of-two
+// FFTs, like the reference backend); the device calls run the B200 shared-memory FFT on
+// the legacy default stream.
 #pragma once
 
 #include <cusignal/detail/zkx_call.h>

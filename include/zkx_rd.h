@@ -15,8 +15,10 @@
  * work is queued.  The last failure's message is available per host thread from
  * zkx_last_error().
  *
- * Transform lengths (nfft) must be powers of two: 1 to 65536 along range (lengths above
- * 16384 run on clusters of two or four CTAs) and 1 to 4096 along pulses (Doppler).
+ * Transform lengths (nfft), along range and along pulses: powers of two from 1 to 65536
+ * (range lengths above 16384 run on clusters of two or four CTAs), and any other length
+ * up to 32768 (Bluestein's chirp-z transform on power-of-two FFTs, as the reference's FFT
+ * backend does for such lengths; its workspace comes from a stream-ordered pool).
  */
 #ifndef ZKX_RD_H
 #define ZKX_RD_H
@@ -161,7 +163,8 @@ ZKX_API int zkx_pulse_doppler_c64(const void* x, int num_pulses, int samples_per
                           float* power, zkx_stream_t stream);
 
 /* Batched complex-to-complex FFT of `batch` contiguous rows of n complex64 (n a power of
- * two, 1..65536); forward unnormalised, inverse scaled by 1/n; x == y allowed.
+ * two up to 65536, or any length up to 32768); forward unnormalised, inverse scaled by 1/n;
+ * x == y allowed.
  * Replaces FFTInterface::fft_batch_device / ifft_batch_device
  * (include/cusignal/backends/fft/fft_interface.h:499-536; fft_interface.cpp:385-470). */
 ZKX_API int zkx_fft_c2c_c64(const void* x, int batch, int n, int inverse, void* y,
@@ -425,7 +428,7 @@ typedef struct {
  * the same replica (device memory, read when the id is first seen with this shape). */
 typedef struct {
     int num_pulses;
-    int samples_per_pulse;   /* a power of two up to 65536 */
+    int samples_per_pulse;   /* and num_pulses: at most 32768, or a power of two up to 65536 */
     uint64_t waveform_id;
     const void* replica;     /* complex64 [replica_length] */
     int replica_length;

@@ -47,11 +47,13 @@ def test_pulse_compression_validation_codes(L):
     assert lib.zkx_pulse_compression_c64(p, 2, 16, p, 4, -1, 1, 7, None, p, None) == L.INVALID_ARGUMENT
     assert lib.zkx_pulse_compression_c64(p, 2, 16, p, 4, -1, 1, 3, None, p, None) == L.INVALID_ARGUMENT
     assert lib.zkx_pulse_compression_c64(p, 2, 16, p, 4, -1, 1, 0, p, p, None) == L.INVALID_ARGUMENT
-    assert lib.zkx_pulse_compression_c64(p, 2, 24, p, 4, -1, 1, 0, None, p, None) == L.UNSUPPORTED_OPERATION
-    # range transforms up to 65536 are supported; 131072 is not
+    # powers of two up to 65536 and any other length up to 32768 are supported
+    assert lib.zkx_pulse_compression_c64(p, 2, 40000, p, 4, -1, 1, 0, None, p, None) == L.UNSUPPORTED_OPERATION
+    assert b"32768" in lib.zkx_last_error()
     assert lib.zkx_pulse_compression_c64(p, 2, 16, p, 4, 1 << 17, 1, 0, None, p, None) == L.UNSUPPORTED_OPERATION
     assert b"65536" in lib.zkx_last_error()
     assert lib.zkx_fft_c2c_c64(p, 2, 1 << 17, 0, p, None) == L.UNSUPPORTED_OPERATION
+    assert lib.zkx_fft_c2c_c64(p, 2, 32769, 0, p, None) == L.UNSUPPORTED_OPERATION
     assert lib.zkx_pulse_compression_c64(None, 2, 16, p, 4, -1, 1, 0, None, p, None) == L.INVALID_ARGUMENT
     assert lib.zkx_pulse_compression_c64(p, 1 << 16, 1 << 16, p, 4, -1, 1, 0, None, p, None) == L.INVALID_SHAPE
     assert b"pulse_compression" in lib.zkx_last_error()
@@ -61,7 +63,8 @@ def test_doppler_and_cfar_validation_codes(L):
     lib = L.lib()
     p = ctypes.c_void_p(16)
     assert lib.zkx_pulse_doppler_c64(p, 0, 8, -1, 0, None, p, None, None) == L.INVALID_SHAPE
-    assert lib.zkx_pulse_doppler_c64(p, 8, 8, 12, 0, None, p, None, None) == L.UNSUPPORTED_OPERATION
+    assert lib.zkx_pulse_doppler_c64(p, 8, 8, 40000, 0, None, p, None, None) == L.UNSUPPORTED_OPERATION
+    assert lib.zkx_pulse_doppler_c64(p, 8, 8, 1 << 17, 0, None, p, None, None) == L.UNSUPPORTED_OPERATION
     assert lib.zkx_pulse_doppler_c64(p, 8, 8, -1, 2, p, p, None, None) == L.INVALID_ARGUMENT
     # window too large for the input: rows <= 2 * (guard + train)
     assert lib.zkx_ca_cfar_f32(p, 2, 20, 100, 2, 2, 8, 8, 1e-3, 0, p, p, None) == L.INVALID_SHAPE

@@ -25,12 +25,13 @@ bool valid_window(int kind, const void* explicit_window)
     return is_explicit == (explicit_window != nullptr);
 }
 
+// Powers of two up to 65536; any other length up to 32768 (chirp-z on power-of-two FFTs).
 int check_transform_length(int nfft, const char* fn)
 {
     if (nfft < 1) return fail(ZKX_INVALID_ARGUMENT, std::string(fn) + ": nfft must be positive");
-    if (!is_pow2(nfft) || nfft > kMaxNfft)
+    if (nfft > kMaxNfft || (!is_pow2(nfft) && nfft > kMaxBluesteinLength))
         return fail(ZKX_UNSUPPORTED_OPERATION,
-                    std::string(fn) + ": nfft must be a power of two no larger than 65536");
+                    std::string(fn) + ": nfft must be at most 32768, or a power of two up to 65536");
     return ZKX_SUCCESS;
 }
 

@@ -414,7 +414,7 @@ int doppler_impl(const float2* x, int pulses, int samples, const float* window, 
     using PL = FftPlan<N, elems_for(N)>;
     constexpr int C = doppler_columns(N);
     const dim3 blocks((samples + C - 1) / C, batch);
-    if (batch > 65535) return fail(ZKX_UNSUPPORTED_OPERATION, "pulse_doppler: more than 65535 CPIs in one batch");
+    if (batch > 65535) return launch_doppler_any(x, pulses, samples, N, window, out, power, batch, s);
     if constexpr (C == 16) {
         // TMA path: rows must be 16-byte multiples and the base 16-byte aligned
         if ((samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
@@ -431,7 +431,8 @@ int doppler_impl(const float2* x, int pulses, int samples, const float* window, 
         }
     }
     const size_t smem = (size_t)C * PL::smem_elems(C < 16) * sizeof(float2);
-    if (smem > 227 * 1024) return fail(ZKX_UNSUPPORTED_OPERATION, "pulse_doppler: nfft above 4096 is not supported");
+    if (smem > 227 * 1024)  // the column tile does not fit: transposed row passes instead
+        return launch_doppler_any(x, pulses, samples, N, window, out, power, batch, s);
     auto k = pulse_doppler_kernel<N>;
     ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<blocks, C * PL::T, smem, s>>>(x, pulses, samples, window, out, power, twiddle_table());
@@ -477,6 +478,9 @@ int launch_replica_spectrum(const float2* replica, int length, int nfft, int nor
                             int window_kind, const float* explicit_window, float2* spectrum,
                             cudaStream_t stream)
 {
+    if (!is_pow2(nfft))
+        return launch_replica_spectrum_any(replica, length, nfft, normalize, window_kind, explicit_window,
+                                           spectrum, stream);
     if (nfft > (1 << kMaxSmemFftLog))
         return launch_long_replica_spectrum(replica, length, nfft, normalize, window_kind, explicit_window,
                                             spectrum, stream);
@@ -496,6 +500,7 @@ int launch_pulse_compression_variant(const float2* x, int pulses, int samples, i
                                      const float2* spectrum, float2* y, int variant, cudaStream_t stream)
 {
     const RowsContiguous src{x, samples};
+    if (!is_pow2(nfft)) return launch_compression_any(src, pulses, samples, nfft, spectrum, y, stream);
     if (nfft > (1 << kMaxSmemFftLog))
         return launch_long_compression(src, pulses, samples, nfft, spectrum, y, stream);
     const bool aligned16 = (samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0;
@@ -519,6 +524,7 @@ int launch_pulse_compression_table(const float2* const* cpis, int count, int pul
         aligned16 = aligned16 && (reinterpret_cast<uintptr_t>(cpis[i]) & 15) == 0;
     }
     const int pulses = count * pulses_per_cpi;
+    if (!is_pow2(nfft)) return launch_compression_any(src, pulses, samples, nfft, spectrum, y, stream);
     if (nfft > (1 << kMaxSmemFftLog))
         return launch_long_compression(src, pulses, samples, nfft, spectrum, y, stream);
 #define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, ZKX_COMPRESSION_DEFAULT, stream)
@@ -529,7 +535,8 @@ int launch_pulse_compression_table(const float2* const* cpis, int count, int pul
 int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft, const float* window,
                          float2* out, float* power, int batch, int columns, cudaStream_t stream)
 {
-    if (nfft > 4096) return fail(ZKX_UNSUPPORTED_OPERATION, "pulse_doppler: nfft above 4096 is not supported");
+    if (!is_pow2(nfft) || nfft > 4096)
+        return launch_doppler_any(x, pulses, samples, nfft, window, out, power, batch, stream);
 #define ZKX_CALL(NN) doppler_impl<NN>(x, pulses, samples, window, out, power, batch, columns, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
 #undef ZKX_CALL
@@ -537,6 +544,7 @@ int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft, con
 
 int launch_fft_rows(const float2* x, int rows, int n, int inverse, float2* y, cudaStream_t stream)
 {
+    if (!is_pow2(n)) return launch_dft_rows(x, rows, n, inverse, y, stream);
     if (n > (1 << kMaxSmemFftLog)) return launch_long_fft_rows(x, rows, n, inverse, y, stream);
 #define ZKX_CALL(NN) fft_rows_impl<NN>(x, rows, inverse, y, stream)
     ZKX_DISPATCH_POW2(ilog2_host(n), ZKX_CALL)

@@ -40,6 +40,7 @@ struct ScratchEntry {
     std::size_t bytes = 0;
 };
 ScratchEntry g_scratch[kMaxDevices][kScratchSlots];
+cudaMemPool_t g_pool[kMaxDevices] = {};
 }  // namespace
 
 void set_error(const std::string& msg) { g_error = msg; }
@@ -145,6 +146,29 @@ int scratch(ScratchSlot slot, std::size_t bytes, void** out)
         e.bytes = bytes;
     }
     *out = e.ptr;
+    return ZKX_SUCCESS;
+}
+
+int stream_workspace(std::size_t bytes, cudaStream_t stream, void** out)
+{
+    int dev = 0;
+    ZKX_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(ZKX_INTERNAL_ERROR, "device index out of range");
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lock(g_mutex);
+        if (!g_pool[dev]) {
+            cudaMemPoolProps props{};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            ZKX_CUDA(cudaMemPoolCreate(&g_pool[dev], &props));
+            std::uint64_t keep = ~std::uint64_t(0);  // keep freed blocks for the next launch
+            ZKX_CUDA(cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+        }
+        pool = g_pool[dev];
+    }
+    ZKX_CUDA(cudaMallocFromPoolAsync(out, bytes, pool, stream));
     return ZKX_SUCCESS;
 }
 

@@ -404,10 +404,12 @@ int validate_request(const zkx_rd_request* r)
         return fail(ZKX_INVALID_ARGUMENT, "rd_submit: null pointer");
     if (r->num_pulses < 1 || r->samples_per_pulse < 1 || r->replica_length < 1)
         return fail(ZKX_INVALID_SHAPE, "rd_submit: shape must be positive");
-    if (!is_pow2(r->samples_per_pulse) || r->samples_per_pulse > 65536 ||
-        !is_pow2(r->num_pulses) || r->num_pulses > 4096)
-        return fail(ZKX_UNSUPPORTED_OPERATION,
-                    "rd_submit: pulses (<= 4096) and samples (<= 65536) must be powers of two");
+    // the plan transforms each CPI at its own extents: powers of two up to 65536, any
+    // other length up to 32768
+    for (int extent : {r->samples_per_pulse, r->num_pulses})
+        if (extent > 65536 || (!is_pow2(extent) && extent > kMaxBluesteinLength))
+            return fail(ZKX_UNSUPPORTED_OPERATION,
+                        "rd_submit: pulses and samples must be at most 32768, or powers of two up to 65536");
     if ((long long)r->num_pulses * r->samples_per_pulse > INT_MAX)
         return fail(ZKX_INVALID_SHAPE, "rd_submit: CPI exceeds kernel capacity");
     return ZKX_SUCCESS;

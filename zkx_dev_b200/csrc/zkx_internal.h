@@ -50,6 +50,22 @@ enum ScratchSlot { kScratchReplica = 0, kScratchDopplerWindow = 1, kScratchCfarI
                    kScratchPolyTaps = 3, kScratchAmbgfun = 4, kScratchSlots = 5 };
 int scratch(ScratchSlot slot, std::size_t bytes, void** out);
 
+// Stream-ordered workspace from the library's per-device pool (memory kept by the pool
+// between uses): valid for work queued on `stream` after the call until released, so
+// concurrent streams never share it.  Usable inside CUDA graph capture.
+int stream_workspace(std::size_t bytes, cudaStream_t stream, void** out);
+struct StreamWorkspace {
+    void* ptr = nullptr;
+    cudaStream_t stream = nullptr;
+    StreamWorkspace() = default;
+    StreamWorkspace(const StreamWorkspace&) = delete;
+    StreamWorkspace& operator=(const StreamWorkspace&) = delete;
+    ~StreamWorkspace()
+    {
+        if (ptr) cudaFreeAsync(ptr, stream);
+    }
+};
+
 bool is_pow2(long long n);
 int ilog2_host(long long n);
 
@@ -107,6 +123,20 @@ int launch_fir(const float* b, int nb, const float* x, int lines, int n, const f
 int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compressed, void* rd,
                         float* power, float* threshold, uint8_t* detections, float* cumulative,
                         cudaStream_t stream, const void* const* table = nullptr);
+// Transforms of any length (bluestein.cu): lengths that are not powers of two up to
+// kMaxBluesteinLength by the chirp-z identity on power-of-two FFTs; spectra in natural order.
+constexpr int kMaxBluesteinLength = 1 << 15;
+int launch_dft_rows(const float2* x, int rows, int n, int inverse, float2* y, cudaStream_t stream);
+int launch_replica_spectrum_any(const float2* replica, int length, int nfft, int normalize, int window_kind,
+                                const float* explicit_window, float2* spectrum, cudaStream_t stream);
+int launch_compression_any(const RowsContiguous& x, int pulses, int samples, int nfft, const float2* spectrum,
+                           float2* y, cudaStream_t stream);
+int launch_compression_any(const RowsTable& x, int pulses, int samples, int nfft, const float2* spectrum,
+                           float2* y, cudaStream_t stream);
+// Doppler transforms of any length up to 32768, and powers of two up to 65536 (transposed
+// row passes; the single-CTA kernels cover powers of two up to 4096).
+int launch_doppler_any(const float2* x, int pulses, int samples, int nfft, const float* window, float2* out,
+                       float* power, int batch, cudaStream_t stream);
 int launch_polyphase(const float* taps, int ntaps, int up, int down, long long offset,
                      const float* x, int lines, int n, float* y, int nout, cudaStream_t stream);
 

@@ -86,9 +86,10 @@ def pulse_compression(x: torch.Tensor, template: torch.Tensor, normalize: bool =
 
 
 def fft(x: torch.Tensor, inverse: bool = False, out: Optional[torch.Tensor] = None) -> torch.Tensor:
-    """Batched C2C transform of the rows of x (complex64 [rows, n], n a power of two up to
-    65536): forward unnormalised, inverse scaled by 1/n (FFTInterface::fft_batch_device /
-    ifft_batch_device).  ``out`` may be x itself."""
+    """Batched C2C transform of the rows of x (complex64 [rows, n]; n a power of two up to
+    65536, or any length up to 32768 by the chirp-z identity, as the reference's FFT
+    backend does for such lengths): forward unnormalised, inverse scaled by 1/n
+    (FFTInterface::fft_batch_device / ifft_batch_device).  ``out`` may be x itself."""
     x = _complex_input(x, 2, "x")
     rows, n = x.shape
     y = torch.empty_like(x) if out is None else out
