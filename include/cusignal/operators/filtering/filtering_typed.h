@@ -1,5 +1,5 @@
 // cusignal_cpp filtering operators on the radar front end -- firfilter, upfirdn,
-// resample_poly -- with the signatures of
+// resample_poly, and the adjacent firfilter2 and hilbert -- with the signatures of
 // ZKX/cusignal_cpp/include/cusignal/operators/filtering/filtering_typed.h (552-567,
 // 745-770), implemented over libzkx_rd.so.  T is one of float, __half, int32_t,
 // int16_t, int8_t; non-float inputs are converted to FP32 on the device first, as the
@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdint>
 #include <numeric>
+#include <optional>
 #include <stdexcept>
 #include <type_traits>
 #include <vector>
@@ -105,6 +106,55 @@ struct FirfilterDeviceResult {
     std::vector<int> y_shape;
     std::vector<int> zf_shape;
     bool has_zf = false;
+};
+
+enum class Firfilter2PadType { odd, even, constant, none };
+enum class Firfilter2Method { pad, gust };
+enum class Firfilter2OutputDtype { fp32, fp64 };
+
+struct Firfilter2Options {
+    std::vector<int> shape;
+    int axis = -1;
+    Firfilter2PadType padtype = Firfilter2PadType::odd;
+    std::optional<int> padlen;
+    Firfilter2Method method = Firfilter2Method::pad;
+    std::optional<int> irlen;  // ignored by the pad method, as in the reference
+};
+
+struct Firfilter2CpuResult {
+    Firfilter2OutputDtype dtype{Firfilter2OutputDtype::fp32};
+    std::vector<float> fp32;
+    std::vector<double> fp64;
+    std::vector<int> shape;
+};
+
+struct Firfilter2DeviceResult {
+    Firfilter2OutputDtype dtype{Firfilter2OutputDtype::fp32};
+    DeviceArray<float> fp32;
+    DeviceArray<double> fp64;
+    std::vector<int> shape;
+};
+
+enum class HilbertOutputDtype { complex_fp32, complex_fp64 };
+
+struct HilbertOptions {
+    std::vector<int> shape;
+    std::optional<int> fft_length;
+    int axis = -1;
+};
+
+struct HilbertCpuResult {
+    HilbertOutputDtype dtype{HilbertOutputDtype::complex_fp32};
+    std::vector<ComplexFloat> complex_fp32;
+    std::vector<ComplexDouble> complex_fp64;
+    std::vector<int> shape;
+};
+
+struct HilbertDeviceResult {
+    HilbertOutputDtype dtype{HilbertOutputDtype::complex_fp32};
+    DeviceArray<ComplexFloat> complex_fp32;
+    DeviceArray<ComplexDouble> complex_fp64;
+    std::vector<int> shape;
 };
 
 namespace detail {
@@ -406,6 +456,82 @@ void resample_poly_device(const DeviceArray<T>& x, int up, int down, ResamplePol
     }
 }
 
+/// Zero-phase FIR along options.axis (filtering_typed.cpp:1226-1302, 1631-1730): padding by
+/// odd / even / constant reflection of padlen samples (default 3 * len(b)), forward and backward
+/// FIR with steady-state initial conditions, crop.  FP32 result; FP64 storage for int32 input.
+/// Odd-reflected pad values keep the rounding / integer wrap of T.
+template <typename T>
+void firfilter2_device(const DeviceArray<T>& b, const DeviceArray<T>& x, Firfilter2DeviceResult& out,
+                       const Firfilter2Options& options = {})
+{
+    if (b.empty()) throw std::invalid_argument("firfilter2 coefficients");
+    if (options.method == Firfilter2Method::gust)
+        throw std::invalid_argument("firfilter2 gust is not supported by cuSignal 23.08.00");
+    if (options.method != Firfilter2Method::pad) throw std::invalid_argument("firfilter2 method");
+    const auto a = detail::axis_layout(x.size(), options.shape, options.axis, "firfilter2");
+    for (int e : a.shape)
+        if (e <= 0) throw std::invalid_argument("firfilter2 input shape");
+    int rounding = ZKX_PAD_ROUND_F32;
+    if constexpr (std::is_same_v<T, __half>) rounding = ZKX_PAD_ROUND_F16;
+    else if constexpr (std::is_same_v<T, std::int8_t>) rounding = ZKX_PAD_ROUND_I8;
+    else if constexpr (std::is_same_v<T, std::int16_t>) rounding = ZKX_PAD_ROUND_I16;
+    else if constexpr (std::is_same_v<T, std::int32_t>) rounding = ZKX_PAD_ROUND_I32;
+    auto bf = detail::staged_f32<T>(b.data(), b.size());
+    auto xf = detail::axis_last(detail::staged_f32<T>(x.data(), x.size()), a);
+    DeviceArray<float> y(x.size());
+    detail::zkx_check(zkx_firfilter2_f32(bf.data(), static_cast<int>(b.size()), xf.data(), (int)a.lines,
+                                         a.samples, static_cast<int>(options.padtype),
+                                         options.padlen.has_value() ? 1 : 0, options.padlen.value_or(0),
+                                         rounding, y.data(), nullptr));
+    y = detail::axis_back(std::move(y), a, a.samples);
+    out.shape = a.shape;
+    if constexpr (std::is_same_v<T, std::int32_t>) {
+        out.dtype = Firfilter2OutputDtype::fp64;
+        out.fp32 = DeviceArray<float>();
+        out.fp64 = detail::widened(y);
+    } else {
+        out.dtype = Firfilter2OutputDtype::fp32;
+        out.fp64 = DeviceArray<double>();
+        cuda_utils::synchronize_stream();
+        out.fp32 = std::move(y);
+    }
+}
+
+/// Analytic signal along options.axis with N = options.fft_length (default the axis length)
+/// (filtering_typed.cpp:500-562, 1819-1872).  ComplexFP32; ComplexFP64 for integer inputs.
+template <typename T>
+void hilbert_device(const DeviceArray<T>& x, HilbertDeviceResult& out, const HilbertOptions& options = {})
+{
+    const auto a = detail::axis_layout(x.size(), options.shape, options.axis, "hilbert");
+    const int nfft = options.fft_length.value_or(a.samples);
+    if (nfft <= 0) throw std::invalid_argument("hilbert N must be positive");
+    auto xf = detail::axis_last(detail::staged_f32<T>(x.data(), x.size()), a);
+    const std::size_t count = static_cast<std::size_t>(a.lines) * static_cast<std::size_t>(nfft);
+    DeviceArray<ComplexFloat> y(count);
+    detail::zkx_check(zkx_hilbert_f32(xf.data(), (int)a.lines, a.samples, nfft, y.data(), nullptr));
+    if (a.transpose) {
+        DeviceArray<ComplexFloat> t(count);
+        detail::zkx_check(zkx_transpose_c64(y.data(), a.shape[1], nfft, t.data(), nullptr));
+        y = std::move(t);
+    }
+    out.shape = a.shape;
+    out.shape[a.axis] = nfft;
+    if constexpr (std::is_integral_v<T>) {
+        out.dtype = HilbertOutputDtype::complex_fp64;
+        out.complex_fp32 = DeviceArray<ComplexFloat>();
+        DeviceArray<ComplexDouble> wide(count);
+        if (count)
+            detail::zkx_check(zkx_widen_f32_to_f64(reinterpret_cast<const float*>(y.data()), 2LL * (long long)count,
+                                                   reinterpret_cast<double*>(wide.data()), nullptr));
+        out.complex_fp64 = std::move(wide);
+    } else {
+        out.dtype = HilbertOutputDtype::complex_fp32;
+        out.complex_fp64 = DeviceArray<ComplexDouble>();
+        cuda_utils::synchronize_stream();
+        out.complex_fp32 = std::move(y);
+    }
+}
+
 // CPU references (declared for callers that link the reference's own CPU implementation).
 template <typename T>
 FirfilterCpuResult firfilter_typed_cpu(const std::vector<T>& b, const std::vector<T>& x,
@@ -413,6 +539,11 @@ FirfilterCpuResult firfilter_typed_cpu(const std::vector<T>& b, const std::vecto
 template <typename T>
 UpfirdnCpuResult upfirdn_typed_cpu(const std::vector<T>& h, const std::vector<T>& x, int up, int down,
                                    const UpfirdnOptions& options = {});
+template <typename T>
+Firfilter2CpuResult firfilter2_typed_cpu(const std::vector<T>& b, const std::vector<T>& x,
+                                         const Firfilter2Options& options = {});
+template <typename T>
+HilbertCpuResult hilbert_typed_cpu(const std::vector<T>& x, const HilbertOptions& options = {});
 template <typename T>
 ResamplePolyCpuResult resample_poly_typed_cpu(const std::vector<T>& x, int up, int down,
                                               const ResamplePolyOptions& options = {},

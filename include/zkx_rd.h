@@ -247,6 +247,43 @@ ZKX_API int zkx_ca_cfar_f32(const float* x, int rank, int rows, int columns, int
 ZKX_API int zkx_fir_f32(const float* b, int nb, const float* x, int lines, int n, const float* zi,
                 float* y, float* zf, zkx_stream_t stream);
 
+/* Padding of zkx_firfilter2_f32, in the order of the reference's Firfilter2PadType
+ * (include/cusignal/operators/filtering/filtering_typed.h, Firfilter2PadType). */
+enum {
+    ZKX_PAD_ODD = 0,
+    ZKX_PAD_EVEN = 1,
+    ZKX_PAD_CONSTANT = 2,
+    ZKX_PAD_NONE = 3
+};
+/* Rounding of an odd-reflected pad value 2*x[edge] - x[reflected]: as the input's element
+ * type does it in the reference (filtering_typed.cpp:1597-1620): float arithmetic, half
+ * (rounded to half), or the 8/16/32-bit integer wrap. */
+enum {
+    ZKX_PAD_ROUND_F32 = 0,
+    ZKX_PAD_ROUND_F16 = 1,
+    ZKX_PAD_ROUND_I8 = 2,
+    ZKX_PAD_ROUND_I16 = 3,
+    ZKX_PAD_ROUND_I32 = 4
+};
+
+/* Zero-phase FIR along the last axis of [lines, n] (n > edge): the line is extended by
+ * edge samples each side (edge = padlen when has_padlen, else 3*nb; 0 for ZKX_PAD_NONE),
+ * filtered forward and backward with steady-state initial conditions, and cropped to n.
+ * At most 4096 coefficients.  Replaces cusignal::firfilter2_device (filtering_typed.h,
+ * firfilter2_device; layout filtering_typed.cpp:1226-1302, algorithm 1631-1730; device
+ * computation filtering_typed.cu:186-286).  Method "gust" is not provided, as in the
+ * reference. */
+ZKX_API int zkx_firfilter2_f32(const float* b, int nb, const float* x, int lines, int n, int padtype,
+                               int has_padlen, int padlen, int pad_rounding, float* y,
+                               zkx_stream_t stream);
+
+/* Analytic signal along the last axis of [lines, n]: x zero-padded or truncated to nfft
+ * (-1 = n), DFT, one-sided mask, inverse DFT; y is complex64 [lines, nfft].  nfft a power
+ * of two up to 65536 or any length up to 32768.  Replaces cusignal::hilbert_device
+ * (filtering_typed.h, hilbert_device; layout filtering_typed.cpp:500-562, algorithm
+ * 1813-1872; device computation filtering_typed.cu:327-352). */
+ZKX_API int zkx_hilbert_f32(const float* x, int lines, int n, int nfft, void* y, zkx_stream_t stream);
+
 /* Output length of upfirdn: floor(((n-1)*up + nh - 1) / down) + 1
  * (src/operators/filtering/filtering_typed.cpp:1091-1098). */
 ZKX_API long long zkx_upfirdn_length(int n, int nh, int up, int down);
@@ -306,6 +343,8 @@ ZKX_API int zkx_cfar_detect_int(const void* x, int dtype, const float* threshold
 /* dst[c, r] = src[r, c] for a row-major [rows, cols] FP32 array (moves a filtering axis
  * last; no counterpart in the reference, whose kernels take axis strides). */
 ZKX_API int zkx_transpose_f32(const float* src, int rows, int cols, float* dst, zkx_stream_t stream);
+/* The same for complex64 elements. */
+ZKX_API int zkx_transpose_c64(const void* src, int rows, int cols, void* dst, zkx_stream_t stream);
 
 /* dst[i] = (double)src[i]: exact widening of FP32 results to the reference's FP64 result
  * storage (src/runtime/fp64_storage_finalize.cu:45-87). */

@@ -76,6 +76,8 @@ def restatement() -> ctypes.CDLL:
         lib.or_ambgfun.argtypes = [_P, _I, _I, _P, _I, _I, _I, _D, _D, _P]
         lib.or_task1_echo.argtypes = [_P, _I, _I, _I, _I, _D, ctypes.c_uint32, _D, _D, _D,
                                       ctypes.c_float, _P, _P]
+        lib.or_firfilter2.argtypes = [_P, _I, _P, _I, _I, _I, _I, _I, _I, _P]
+        lib.or_hilbert.argtypes = [_P, _I, _I, _I, _P]
         _lib_cache["r"] = lib
     return _lib_cache["r"]
 
@@ -96,6 +98,8 @@ def reference() -> Optional[ctypes.CDLL]:
         lib.zkx_ref_resample_poly_f32.argtypes = [_P, _I, _I, _I, _I, _D, _P, _I, _P, _P, _P]
         lib.zkx_ref_firwin_kaiser.argtypes = [_I, _D, _D, _P]
         lib.zkx_ref_ambgfun_f32.argtypes = [_P, _I, _I, _P, _I, _I, _I, _D, _D, _P, _P]
+        lib.zkx_ref_firfilter2.argtypes = [_I, _P, _I, _P, _P, _I, _I, _I, _I, _I, _P, _P]
+        lib.zkx_ref_hilbert.argtypes = [_I, _P, _P, _I, _I, _I, _I, _P, _P]
         _lib_cache["ref"] = lib
     return _lib_cache["ref"]
 
@@ -460,3 +464,68 @@ def task1_echo(waveform, pulses: int, samples: int, delay: int, doppler_hz: floa
     _check(restatement().or_task1_echo(_ptr(w), w.size, pulses, samples, delay, doppler_hz, seed, prf, fs,
                                        amplitude, noise_std, _ptr(noiseless), _ptr(noise)))
     return noiseless, noise
+
+
+# ------------------------------------------------------------ firfilter2 / hilbert
+
+PADTYPE = {"odd": 0, "even": 1, "constant": 2, "none": 3}
+# element types of the reference's instantiations, with the odd-pad rounding each implies
+_REF_DTYPE = {np.dtype(np.float32): 0, np.dtype(np.float16): 1, np.dtype(np.int32): 2,
+              np.dtype(np.int16): 3, np.dtype(np.int8): 4}
+PAD_ROUNDING = {np.dtype(np.float32): 0, np.dtype(np.float16): 1, np.dtype(np.int8): 2,
+                np.dtype(np.int16): 3, np.dtype(np.int32): 4}
+
+
+def firfilter2(b, x, padtype: str = "odd", padlen: Optional[int] = None, rounding: int = 0) -> np.ndarray:
+    """The C restatement along the last axis of x [lines, n] (float values); double result."""
+    b, x = _f32(b), _f32(x)
+    x2 = x.reshape(-1, x.shape[-1])
+    out = np.zeros(x2.shape, dtype=np.float64)
+    _check(restatement().or_firfilter2(b.ctypes.data, b.size, x2.ctypes.data, x2.shape[0], x2.shape[1],
+                                       PADTYPE[padtype], int(padlen is not None), padlen or 0, rounding,
+                                       out.ctypes.data))
+    return out.reshape(x.shape)
+
+
+def ref_firfilter2(b, x, axis: int = -1, padtype: str = "odd", padlen: Optional[int] = None):
+    """The reference's firfilter2_typed_cpu<T> for T = x.dtype (b is cast to it); returns
+    (result as double, is_fp64)."""
+    lib = reference()
+    if lib is None:
+        raise OracleError("reference library not built")
+    x = np.ascontiguousarray(x)
+    b = np.ascontiguousarray(np.asarray(b).astype(x.dtype))
+    shape = np.asarray(x.shape, dtype=np.int32)
+    out = np.zeros(x.shape, dtype=np.float64)
+    is64 = ctypes.c_int(0)
+    _check(lib.zkx_ref_firfilter2(_REF_DTYPE[x.dtype], b.ctypes.data, b.size, x.ctypes.data, shape.ctypes.data,
+                                  x.ndim, axis, PADTYPE[padtype], int(padlen is not None), padlen or 0,
+                                  out.ctypes.data, ctypes.byref(is64)), lib)
+    return out, bool(is64.value)
+
+
+def hilbert(x, nfft: Optional[int] = None) -> np.ndarray:
+    """The C restatement along the last axis of x [lines, n]; complex128 [lines, nfft]."""
+    x = _f32(x)
+    x2 = x.reshape(int(np.prod(x.shape[:-1])), x.shape[-1])
+    nf = x2.shape[1] if nfft is None else nfft
+    out = np.zeros((x2.shape[0], nf), dtype=np.complex128)
+    _check(restatement().or_hilbert(x2.ctypes.data, x2.shape[0], x2.shape[1], nf, out.ctypes.data))
+    return out.reshape(x.shape[:-1] + (nf,))
+
+
+def ref_hilbert(x, nfft: Optional[int] = None, axis: int = -1):
+    """The reference's hilbert_typed_cpu<T> for T = x.dtype; returns (complex128, is_fp64)."""
+    lib = reference()
+    if lib is None:
+        raise OracleError("reference library not built")
+    x = np.ascontiguousarray(x)
+    shape = np.asarray(x.shape, dtype=np.int32)
+    ax = axis % x.ndim
+    out_shape = list(x.shape)
+    out_shape[ax] = x.shape[ax] if nfft is None else nfft
+    out = np.zeros(out_shape, dtype=np.complex128)
+    is64 = ctypes.c_int(0)
+    _check(lib.zkx_ref_hilbert(_REF_DTYPE[x.dtype], x.ctypes.data, shape.ctypes.data, x.ndim, axis,
+                               int(nfft is not None), nfft or 0, out.ctypes.data, ctypes.byref(is64)), lib)
+    return out, bool(is64.value)

@@ -658,3 +658,145 @@ int or_task1_echo(const float* waveform, int L, int P, int N, int delay, double 
     }
     return OR_OK;
 }
+
+/* ---------------------------------------------------------------- firfilter2 */
+
+/* f rounded to the nearest binary16 value (ties to even; infinity past 65520), as a float. */
+static float or_round_half(float f)
+{
+    if (isnan(f)) return f;
+    const float a = fabsf(f);
+    if (a >= 65520.0f) return copysignf(INFINITY, f);
+    double quantum;
+    if (a < 6.103515625e-05f) {
+        quantum = ldexp(1.0, -24);            /* subnormal spacing */
+    } else {
+        int e;
+        frexpf(a, &e);                        /* a in [2^(e-1), 2^e): 11 significant bits */
+        quantum = ldexp(1.0, e - 11);
+    }
+    return copysignf((float)(nearbyint((double)a / quantum) * quantum), f);
+}
+
+/* filtering_typed.cpp:1597-1620: 2 * endpoint - reflected in the element type. */
+static float or_odd_reflect(float endpoint, float reflected, int rounding)
+{
+    if (rounding == 1) {
+        const float doubled = or_round_half(2.0f * endpoint);
+        return or_round_half(doubled - reflected);
+    }
+    if (rounding >= 2 && rounding <= 4) {
+        const int bits = rounding == 2 ? 8 : rounding == 3 ? 16 : 32;
+        const long long modulus = 1LL << bits, sign = modulus / 2;
+        long long v = 2LL * (long long)endpoint - (long long)reflected;
+        v %= modulus;
+        if (v < 0) v += modulus;
+        if (v >= sign) v -= modulus;
+        return (float)v;
+    }
+    const float doubled = 2.0f * endpoint;
+    return doubled - reflected;
+}
+
+/* One causal pass with the steady-state initial state: out[i] = state[i] * scale (i < nb-1)
+ * + sum_k b[k] in[i-k], state[s] = b[s+1] + ... + b[nb-1] (filtering_typed.cpp:1645-1664). */
+static void or_fir_steady(const double* b, int nb, const double* state, const double* in, int count,
+                          double scale, double* out)
+{
+    for (int i = 0; i < count; ++i) {
+        double v = i < nb - 1 ? state[i] * scale : 0.0;
+        for (int k = 0; k < nb; ++k)
+            if (i - k >= 0) v += b[k] * in[i - k];
+        out[i] = v;
+    }
+}
+
+int or_firfilter2(const float* b, int nb, const float* x, int lines, int n, int padtype, int has_padlen,
+                  int padlen, int rounding, double* out)
+{
+    if (nb < 1 || padtype < 0 || padtype > 3 || lines < 0 || n < 1) return OR_INVALID;
+    int requested = 0;
+    if (padtype != 3) requested = has_padlen ? padlen : 3 * nb;
+    if (n <= requested) return OR_INVALID;
+    const int edge = requested > 0 ? requested : 0;
+    const int ne = n + 2 * edge;
+    double* bd = malloc(sizeof(double) * nb);
+    double* state = malloc(sizeof(double) * (nb > 1 ? nb - 1 : 1));
+    double* e = malloc(sizeof(double) * ne);
+    double* f = malloc(sizeof(double) * ne);
+    double* g = malloc(sizeof(double) * ne);
+    if (!bd || !state || !e || !f || !g) {
+        free(bd); free(state); free(e); free(f); free(g);
+        return OR_INVALID;
+    }
+    for (int k = 0; k < nb; ++k) bd[k] = b[k];
+    double suffix = 0.0;
+    for (int s = nb - 2; s >= 0; --s) {
+        suffix += bd[s + 1];
+        state[s] = suffix;
+    }
+    for (int line = 0; line < lines; ++line) {
+        const float* xl = x + (size_t)line * n;
+        for (int i = 0; i < ne; ++i) {
+            float v;
+            if (i < edge) {
+                const float r = xl[edge - i];
+                v = padtype == 0 ? or_odd_reflect(xl[0], r, rounding) : padtype == 1 ? r : xl[0];
+            } else if (i < edge + n) {
+                v = xl[i - edge];
+            } else {
+                const float r = xl[n - 2 - (i - edge - n)];
+                v = padtype == 0 ? or_odd_reflect(xl[n - 1], r, rounding) : padtype == 1 ? r : xl[n - 1];
+            }
+            e[i] = v;
+        }
+        or_fir_steady(bd, nb, state, e, ne, e[0], f);
+        /* backward pass on the reversed forward output, scaled by its first (= last) value */
+        for (int i = 0; i < ne; ++i) e[i] = f[ne - 1 - i];
+        or_fir_steady(bd, nb, state, e, ne, e[0], g);
+        for (int m = 0; m < n; ++m) out[(size_t)line * n + m] = g[ne - 1 - (edge + m)];
+    }
+    free(bd); free(state); free(e); free(f); free(g);
+    return OR_OK;
+}
+
+/* ---------------------------------------------------------------- hilbert */
+
+int or_hilbert(const float* x, int lines, int n, int nfft, double* out)
+{
+    /* the reference's direct double sums, phase evaluated per term as in
+       filtering_typed.cpp:1838-1870 */
+    if (lines < 0 || n < 0 || nfft < 1) return OR_INVALID;
+    const double two_pi = 6.283185307179586476925286766559;
+    double* spec = malloc(sizeof(double) * 2 * nfft);
+    if (!spec) return OR_INVALID;
+    for (int line = 0; line < lines; ++line) {
+        const float* xl = x + (size_t)line * n;
+        for (int k = 0; k < nfft; ++k) {
+            double re = 0.0, im = 0.0;
+            for (int j = 0; j < nfft; ++j) {
+                const double value = j < n ? (double)xl[j] : 0.0;
+                const double angle = -two_pi * k * j / nfft;
+                re += value * cos(angle);
+                im += value * sin(angle);
+            }
+            const double w = (k == 0 || ((nfft % 2) == 0 && k == nfft / 2)) ? 1.0
+                           : (k < (nfft + 1) / 2 ? 2.0 : 0.0);
+            spec[2 * k] = re * w;
+            spec[2 * k + 1] = im * w;
+        }
+        double* ol = out + (size_t)2 * line * nfft;
+        for (int m = 0; m < nfft; ++m) {
+            double re = 0.0, im = 0.0;
+            for (int k = 0; k < nfft; ++k) {
+                const double angle = two_pi * k * m / nfft;
+                re += spec[2 * k] * cos(angle) - spec[2 * k + 1] * sin(angle);
+                im += spec[2 * k] * sin(angle) + spec[2 * k + 1] * cos(angle);
+            }
+            ol[2 * m] = re / nfft;
+            ol[2 * m + 1] = im / nfft;
+        }
+    }
+    free(spec);
+    return OR_OK;
+}

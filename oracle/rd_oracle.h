@@ -128,6 +128,19 @@ int or_task1_echo(const float* waveform, int pulse_samples, int num_pulses, int 
                   int delay, double doppler_hz, uint32_t seed, double prf, double sample_rate,
                   double amplitude, float noise_std, double* noiseless, float* noise);
 
+/* firfilter2 (filtering_typed.cpp:1226-1302 layout, 1631-1730 algorithm) along the last
+ * axis of x [lines, n]: odd/even/constant/none padding by edge (padlen, default 3 nb), the
+ * odd pad value 2 x0 - x[r] rounded as `rounding` says (0 float, 1 half, 2/3/4 the 8/16/32
+ * bit integer wrap), forward and backward FIR with steady-state initial conditions in
+ * double, crop.  out [lines, n] double.  Returns OR_INVALID on the reference's errors. */
+int or_firfilter2(const float* b, int nb, const float* x, int lines, int n, int padtype, int has_padlen,
+                  int padlen, int rounding, double* out);
+
+/* hilbert (filtering_typed.cpp:500-562 layout, 1819-1872 algorithm) along the last axis of
+ * x [lines, n]: zero-pad/truncate to nfft, direct double DFT, one-sided mask, direct
+ * inverse DFT.  out [lines, nfft] complex, interleaved double. */
+int or_hilbert(const float* x, int lines, int n, int nfft, double* out);
+
 #ifdef __cplusplus
 }
 #endif

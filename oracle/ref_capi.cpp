@@ -19,6 +19,8 @@
 //   firwin_typed_cpu             include/cusignal/operators/filter_design/filter_design_typed.h:132
 //   kaiser_typed_cpu             include/cusignal/operators/windows/windows_typed.h:169
 //   ambgfun_typed_cpu            src/operators/radartools/radartools_typed.cpp:330-463
+//   firfilter2_typed_cpu         src/operators/filtering/filtering_typed.cpp:1631-1730
+//   hilbert_typed_cpu            src/operators/filtering/filtering_typed.cpp:1819-1872
 #include <cusignal/operators/radartools/radartools_typed.h>
 #include <cusignal/operators/filtering/filtering_typed.h>
 #include <cusignal/operators/filter_design/filter_design_typed.h>
@@ -268,5 +270,101 @@ extern "C" int zkx_ref_ambgfun_f32(const float* x, int x_count, int nx, const fl
         } else {
             for (std::size_t i = 0; i < r.fp32.size(); ++i) out[i] = r.fp32[i];
         }
+    });
+}
+
+// firfilter2_typed_cpu<T> and hilbert_typed_cpu<T> for the element types the reference
+// instantiates (dtype 0 float, 1 __half, 2 int32, 3 int16, 4 int8; b and x hold raw
+// elements of that type).  x has row-major `shape` (rank entries) and is filtered along
+// `axis`; results are widened to double (complex results interleaved), *is_fp64 tells
+// whether the reference produced FP64 storage.
+//   firfilter2_typed_cpu   src/operators/filtering/filtering_typed.cpp:1631-1730
+//   hilbert_typed_cpu      src/operators/filtering/filtering_typed.cpp:1819-1872
+namespace {
+template <class T>
+std::vector<T> typed_vector(const void* p, std::size_t n)
+{
+    const T* t = static_cast<const T*>(p);
+    return std::vector<T>(t, t + n);
+}
+
+template <class T>
+void run_firfilter2(const void* b, int nb, const void* x, const int* shape, int rank, int axis,
+                    int padtype, int has_padlen, int padlen, double* out, int* is_fp64)
+{
+    cusignal::Firfilter2Options o;
+    std::size_t count = 1;
+    for (int i = 0; i < rank; ++i) {
+        o.shape.push_back(shape[i]);
+        count *= static_cast<std::size_t>(shape[i]);
+    }
+    o.axis = axis;
+    o.padtype = static_cast<cusignal::Firfilter2PadType>(padtype);
+    if (has_padlen) o.padlen = padlen;
+    const auto r = cusignal::firfilter2_typed_cpu<T>(typed_vector<T>(b, nb), typed_vector<T>(x, count), o);
+    *is_fp64 = r.dtype == cusignal::Firfilter2OutputDtype::fp64 ? 1 : 0;
+    if (*is_fp64) std::memcpy(out, r.fp64.data(), r.fp64.size() * sizeof(double));
+    else for (std::size_t i = 0; i < r.fp32.size(); ++i) out[i] = r.fp32[i];
+}
+
+template <class T>
+void run_hilbert(const void* x, const int* shape, int rank, int axis, int has_n, int n, double* out,
+                 int* is_fp64)
+{
+    cusignal::HilbertOptions o;
+    std::size_t count = 1;
+    for (int i = 0; i < rank; ++i) {
+        o.shape.push_back(shape[i]);
+        count *= static_cast<std::size_t>(shape[i]);
+    }
+    o.axis = axis;
+    if (has_n) o.fft_length = n;
+    const auto r = cusignal::hilbert_typed_cpu<T>(typed_vector<T>(x, count), o);
+    *is_fp64 = r.dtype == cusignal::HilbertOutputDtype::complex_fp64 ? 1 : 0;
+    if (*is_fp64) {
+        for (std::size_t i = 0; i < r.complex_fp64.size(); ++i) {
+            out[2 * i] = r.complex_fp64[i].re;
+            out[2 * i + 1] = r.complex_fp64[i].im;
+        }
+    } else {
+        for (std::size_t i = 0; i < r.complex_fp32.size(); ++i) {
+            out[2 * i] = r.complex_fp32[i].re;
+            out[2 * i + 1] = r.complex_fp32[i].im;
+        }
+    }
+}
+
+template <class F>
+void by_dtype(int dtype, F&& f)
+{
+    switch (dtype) {
+    case 0: f(float{}); break;
+    case 1: f(__half{}); break;
+    case 2: f(std::int32_t{}); break;
+    case 3: f(std::int16_t{}); break;
+    case 4: f(std::int8_t{}); break;
+    default: throw std::invalid_argument("dtype");
+    }
+}
+}  // namespace
+
+extern "C" int zkx_ref_firfilter2(int dtype, const void* b, int nb, const void* x, const int* shape, int rank,
+                                  int axis, int padtype, int has_padlen, int padlen, double* out,
+                                  int* is_fp64)
+{
+    return guarded([&] {
+        by_dtype(dtype, [&](auto tag) {
+            run_firfilter2<decltype(tag)>(b, nb, x, shape, rank, axis, padtype, has_padlen, padlen, out, is_fp64);
+        });
+    });
+}
+
+extern "C" int zkx_ref_hilbert(int dtype, const void* x, const int* shape, int rank, int axis, int has_n, int n,
+                               double* out, int* is_fp64)
+{
+    return guarded([&] {
+        by_dtype(dtype, [&](auto tag) {
+            run_hilbert<decltype(tag)>(x, shape, rank, axis, has_n, n, out, is_fp64);
+        });
     });
 }

@@ -1,7 +1,8 @@
 // Drives the cusignal:: C++ API (include/cusignal/...) the way the reference's callers
 // do -- pulse compression, resident pulse Doppler, cfar_alpha, CA-CFAR, firfilter,
-// upfirdn, resample_poly, the batched FFT -- on inputs read from <dir>/*.bin and writes
+// upfirdn, resample_poly, firfilter2, hilbert, the batched FFT -- on inputs read from <dir>/*.bin and writes
 // every result to <dir>/out_*.bin for tests/test_gpu_dropin.py to check.
+#include <cusignal/operators/filtering/filtering_typed.h>
 #include <cusignal/operators/radartools/radartools_typed.h>
 #include <cusignal/runtime/cuda_utils.h>
 
@@ -129,6 +130,46 @@ int main(int argc, char** argv)
         UpfirdnDeviceResult uri;
         upfirdn_device(hi, si, 2, 3, uri);
         save("upfirdn_i16", uri.fp32.to_host());
+
+        // zero-phase FIR (default odd padding; int16 with even padding along axis 0) and the
+        // analytic signal (length 5000, and an int16 input along axis 0)
+        Firfilter2DeviceResult f2;
+        firfilter2_device(b, s, f2);
+        if (f2.dtype != Firfilter2OutputDtype::fp32) throw std::runtime_error("firfilter2 of float is FP32");
+        save("fir2", f2.fp32.to_host());
+        auto b16 = DeviceArray<std::int16_t>::from_host(std::vector<std::int16_t>{1, 2, 1});
+        Firfilter2Options f2o;
+        f2o.shape = {NF / 8, 8};
+        f2o.axis = 0;
+        f2o.padtype = Firfilter2PadType::even;
+        f2o.padlen = 20;
+        Firfilter2DeviceResult f2i;
+        firfilter2_device(b16, si, f2i, f2o);
+        save("fir2_i16_axis0", f2i.fp32.to_host());
+        bool gust_threw = false;
+        try {
+            Firfilter2Options g;
+            g.method = Firfilter2Method::gust;
+            Firfilter2DeviceResult bad;
+            firfilter2_device(b, s, bad, g);
+        } catch (const std::invalid_argument&) {
+            gust_threw = true;
+        }
+        if (!gust_threw) throw std::runtime_error("firfilter2 gust did not throw");
+        HilbertOptions ho;
+        ho.fft_length = 5000;
+        HilbertDeviceResult hr;
+        hilbert_device(s, hr, ho);
+        if (hr.dtype != HilbertOutputDtype::complex_fp32 || hr.shape[0] != 5000)
+            throw std::runtime_error("hilbert of float is ComplexFP32 [N]");
+        save("hilbert", hr.complex_fp32.to_host());
+        HilbertOptions hio;
+        hio.shape = {NF / 8, 8};
+        hio.axis = 0;
+        HilbertDeviceResult hri;
+        hilbert_device(si, hri, hio);
+        if (hri.dtype != HilbertOutputDtype::complex_fp64) throw std::runtime_error("hilbert of int16 is ComplexFP64");
+        save("hilbert_i16_axis0", hri.complex_fp64.to_host());
 
         // batched FFT round trip
         FFTInterface fft(N, FFTInterface::BatchOnly{});

@@ -5,7 +5,8 @@ for every operator probe run, the probe command line (``*_full.log``) and a raw 
 with ``typed_input_manifest`` (SHA-256 of each input array) and ``cpu_output_digest``
 (SHA-256 of the flattened output of the reference's ``*_typed_cpu`` function).  The
 probe inputs are deterministic functions of the command-line arguments, so the oracle
-can regenerate them and must reproduce both digests bit for bit.
+can regenerate them and must reproduce both digests bit for bit.  firfilter2 and
+hilbert (the remaining-operators probes) keep every element type.
 
 This script reads the archive in place (it needs the reference checkout) and writes
 ``published_digests.json`` beside itself; tests/test_oracle_published.py consumes that
@@ -22,7 +23,10 @@ import os
 import shlex
 
 OPS = ["pulse_compression", "pulse_doppler", "ca_cfar", "cfar_alpha", "upfirdn",
-       "resample_poly", "firfilter"]
+       "resample_poly", "firfilter", "firfilter2", "hilbert"]
+# operators whose cases are kept for every element type (their padding / output storage
+# depends on it); the others keep FP32 only
+ALL_DTYPES = {"firfilter2", "hilbert"}
 ARCHIVE = os.path.join("plot_in_report", "0817结果", "0817结果（含耗时）", "04_算子结果")
 
 
@@ -51,7 +55,7 @@ def main() -> None:
                                     recursive=True)):
             with open(raw, encoding="utf-8") as fh:
                 d = json.load(fh)
-            if d.get("requested_dtype") != "FP32":
+            if d.get("requested_dtype") != "FP32" and op not in ALL_DTYPES:
                 continue
             logs = glob.glob(os.path.join(os.path.dirname(raw), "*_full.log"))
             if not logs:

@@ -27,6 +27,17 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
+def hilbert64(x, nfft):
+    """Analytic signal along the last axis in FP64 (the same mask as the restatement)."""
+    X = np.fft.fft(np.asarray(x, dtype=np.float64), n=nfft, axis=-1)
+    w = np.zeros(nfft)
+    w[0] = 1.0
+    w[1:(nfft + 1) // 2] = 2.0
+    if nfft % 2 == 0:
+        w[nfft // 2] = 1.0
+    return np.fft.ifft(X * w, axis=-1)
+
+
 def test_dropin_headers_compile_and_link():
     """The headers compile as C++17 with nvcc and the probe links against the library
     (no GPU needed)."""
@@ -105,6 +116,16 @@ def test_dropin_api_matches_oracle():
             got = out(name, np.float64)
             ref = O.ambgfun(t, fs=2.0, cut=cut, cut_value=cv)
             assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= REL_L2, name
+        assert rel(out("fir2", np.float32), O.firfilter2(b, s)) <= REL_L2
+        fir2i = out("fir2_i16_axis0", np.float32).reshape(NF // 8, 8)
+        ref2i = O.firfilter2(np.array([1, 2, 1], np.float32), si.astype(np.float32).reshape(NF // 8, 8).T.copy(),
+                             "even", 20, O.PAD_ROUNDING[np.dtype(np.int16)]).T
+        assert rel(fir2i, ref2i) <= REL_L2
+        hil = out("hilbert", np.float32).view(np.complex64)
+        assert hil.size == 5000
+        assert rel(hil, hilbert64(s, 5000)) <= REL_L2
+        hili = out("hilbert_i16_axis0", np.float64).view(np.complex128).reshape(NF // 8, 8)
+        assert rel(hili, hilbert64(si.astype(np.float32).reshape(NF // 8, 8).T, NF // 8).T) <= REL_L2
         spec = out("fft", np.float32).view(np.complex64).reshape(P, N)
         assert rel(spec, np.fft.fft(x.astype(np.complex128), axis=1)) <= REL_L2
         assert rel(out("ifft", np.float32).view(np.complex64).reshape(P, N), x) <= 1e-6

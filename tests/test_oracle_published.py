@@ -11,6 +11,13 @@ Probe sources restated (paths within ZKX/test_all/operators):
   cases/filtering/upfirdn/operator_probe.cu:23,25         (make, h seed+1)
   cases/filtering/resample_poly/operator_probe.cu:27-28   (input, custom taps 1,2,3,2,1)
   shared/filtering/task2_filter_probe.cu:28               (signal seed 29, taps)
+  cases/filtering/firfilter2/operator_probe.cu:26,32       (input, taps 1,1,1)
+  cases/filtering/hilbert/operator_probe.cu:38,48          (input, N = axis length)
+
+firfilter2 and hilbert cases cover every element type the reference instantiates; the
+restatement runs on the values as float with the element type's odd-pad rounding, and
+its double result is stored as the reference stores it (FP32, or FP64 for int32 /
+integral hilbert inputs).
 """
 from __future__ import annotations
 
@@ -76,6 +83,19 @@ def fir_signal(n: int, seed: int) -> np.ndarray:
 
 def fir_taps(n: int) -> np.ndarray:
     return np.array([4 if i == n // 2 else (1 if i % 2 else 0) for i in range(n)], dtype=np.float32)
+
+
+_PROBE_DTYPES = {"FP32": np.float32, "FP16": np.float16, "INT32": np.int32, "INT16": np.int16,
+                 "INT8": np.int8}
+
+
+def remaining_input(n: int, seed: int, mult: int, mod: int, dtype) -> np.ndarray:
+    """x[i] = ((i*mult + seed) % mod - mod//2), times 0.25 for floating element types."""
+    i = np.arange(n, dtype=np.int64)
+    r = ((i * mult + seed) % mod) - mod // 2
+    if np.issubdtype(dtype, np.integer):
+        return r.astype(dtype)
+    return (r.astype(np.float32) * np.float32(0.25)).astype(dtype)
 
 
 def interleave(z: np.ndarray) -> np.ndarray:
@@ -150,6 +170,24 @@ def run_case(case):
         b, x = fir_taps(taps), fir_signal(n, 29)
         got_in = {"b": sha(b), "x": sha(x)}
         out = O.firfilter(b, x).astype(np.float32)
+    elif op == "firfilter2":
+        dt = _PROBE_DTYPES[a["dtype"]]
+        rows, cols, axis, seed = int(a["rows"]), int(a["cols"]), int(a["axis"]), int(a["seed"])
+        x = remaining_input(rows * cols, seed, 13, 9, dt)
+        b = np.ones(3, dtype=dt)
+        got_in = {"x": sha(x), "b": sha(b)}
+        rounding = O.PAD_ROUNDING[np.dtype(dt)]
+        y = along_axis(lambda v: O.firfilter2(b.astype(np.float32), v, a["padtype"], int(a["padlen"]), rounding),
+                       x.astype(np.float32).reshape(rows, cols), axis)
+        out = y.reshape(-1).astype(np.float64 if dt == np.int32 else np.float32)
+    elif op == "hilbert":
+        dt = _PROBE_DTYPES[a["dtype"]]
+        rows, cols, axis, seed = int(a["rows"]), int(a["cols"]), int(a["axis"]), int(a["seed"])
+        x = remaining_input(rows * cols, seed, 17, 23, dt)
+        got_in = {"x": sha(x)}
+        y = along_axis(lambda v: O.hilbert(v), x.astype(np.float32).reshape(rows, cols), axis)
+        out = np.stack([y.real, y.imag], axis=-1).reshape(-1)
+        out = out.astype(np.float64 if np.issubdtype(dt, np.integer) else np.float32)
     else:
         raise AssertionError(op)
     return want_in, got_in, out

@@ -21,6 +21,8 @@ OUT_OF_MEMORY = 2003
 WINDOW_NONE, WINDOW_HANN, WINDOW_HAMMING, WINDOW_EXPLICIT_FP32, WINDOW_EXPLICIT_FP64 = range(5)
 CFAR_ACCURATE, CFAR_COMPAT = 0, 1
 PRECISION_FP32, PRECISION_TC_F16, PRECISION_TC_BF16 = 0, 1, 2
+PAD_ODD, PAD_EVEN, PAD_CONSTANT, PAD_NONE = range(4)
+PAD_ROUND_F32, PAD_ROUND_F16, PAD_ROUND_I8, PAD_ROUND_I16, PAD_ROUND_I32 = range(5)
 
 # Every symbol the header declares, with its ctypes signature.
 _P = ctypes.c_void_p
@@ -91,6 +93,8 @@ SIGNATURES = {
     "zkx_cfar_reference_count": (_I, [_I, _I, _I, _I, _I]),
     "zkx_ca_cfar_f32": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _D, _I, _P, _P, _P]),
     "zkx_fir_f32": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P]),
+    "zkx_firfilter2_f32": (_I, [_P, _I, _P, _I, _I, _I, _I, _I, _I, _P, _P]),
+    "zkx_hilbert_f32": (_I, [_P, _I, _I, _I, _P, _P]),
     "zkx_upfirdn_length": (ctypes.c_longlong, [_I, _I, _I, _I]),
     "zkx_upfirdn_f32": (_I, [_P, _I, _P, _I, _I, _I, _I, _P, _P]),
     "zkx_resample_poly_layout": (_I, [_I, _I, _I, _I, _I, ctypes.POINTER(ResampleLayout)]),
@@ -100,6 +104,7 @@ SIGNATURES = {
     "zkx_widen_f32_to_f64": (_I, [_P, ctypes.c_longlong, _P, _P]),
     "zkx_cfar_detect_int": (_I, [_P, _I, _P, ctypes.c_longlong, _P, _P]),
     "zkx_transpose_f32": (_I, [_P, _I, _I, _P, _P]),
+    "zkx_transpose_c64": (_I, [_P, _I, _I, _P, _P]),
     "zkx_resample_poly_design_window": (_I, [ctypes.POINTER(ResampleLayout), _P, _P]),
     "zkx_rd_plan_create": (_I, [ctypes.POINTER(RdDesc), _P, _P, _P, _P, ctypes.POINTER(_P)]),
     "zkx_rd_plan_destroy": (_I, [_P]),

@@ -95,9 +95,10 @@ __global__ void detect_int_kernel(const T* __restrict__ x, const float* __restri
 }
 
 // 32 x 32 tiles through shared memory: coalesced reads and writes.
-__global__ void transpose_kernel(const float* __restrict__ src, int rows, int cols, float* __restrict__ dst)
+template <class T>
+__global__ void transpose_kernel(const T* __restrict__ src, int rows, int cols, T* __restrict__ dst)
 {
-    __shared__ float tile[32][33];
+    __shared__ T tile[32][33];
     const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
     for (int i = threadIdx.y; i < 32; i += blockDim.y) {
         const int r = r0 + i, c = c0 + threadIdx.x;
@@ -139,14 +140,27 @@ extern "C" int zkx_cfar_detect_int(const void* x, int dtype, const float* thresh
     return ZKX_SUCCESS;
 }
 
-extern "C" int zkx_transpose_f32(const float* src, int rows, int cols, float* dst, zkx_stream_t stream)
+namespace {
+template <class T>
+int transpose(const T* src, int rows, int cols, T* dst, cudaStream_t stream)
 {
     if (rows < 0 || cols < 0) return fail(ZKX_INVALID_SHAPE, "transpose: negative extent");
     if ((long long)rows * cols == 0) return ZKX_SUCCESS;
     if (!src || !dst || src == dst) return fail(ZKX_INVALID_ARGUMENT, "transpose: null or aliased pointer");
     if ((rows + 31) / 32 > 65535) return fail(ZKX_UNSUPPORTED_OPERATION, "transpose: too many rows");
     dim3 grid((cols + 31) / 32, (rows + 31) / 32);
-    transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(src, rows, cols, dst);
+    transpose_kernel<T><<<grid, dim3(32, 8), 0, stream>>>(src, rows, cols, dst);
     ZKX_LAUNCHED("transpose_kernel");
     return ZKX_SUCCESS;
+}
+}  // namespace
+
+extern "C" int zkx_transpose_f32(const float* src, int rows, int cols, float* dst, zkx_stream_t stream)
+{
+    return transpose(src, rows, cols, dst, stream);
+}
+
+extern "C" int zkx_transpose_c64(const void* src, int rows, int cols, void* dst, zkx_stream_t stream)
+{
+    return transpose(static_cast<const float2*>(src), rows, cols, static_cast<float2*>(dst), stream);
 }

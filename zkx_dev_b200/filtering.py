@@ -1,4 +1,4 @@
-"""Front-end filters on the B200: firfilter, upfirdn, resample_poly.
+"""Front-end filters on the B200: firfilter, upfirdn, resample_poly, firfilter2, hilbert.
 
 Mirrors the reference's operator interface (cuSignal 23.08 ``filtering/filtering.py:109``
 ``firfilter(b, x, axis=-1, zi=None)``, ``filtering/resample.py:304,448`` ``resample_poly``
@@ -146,4 +146,54 @@ def resample_poly(x: torch.Tensor, up: int, down: int, axis: int = 0, window=("k
     y = torch.empty(xm.shape[:-1] + (lay.output_samples,), dtype=torch.float32, device=x.device)
     L.check(L.lib().zkx_resample_poly_f32(xm.data_ptr(), lines, n, ctypes.byref(lay),
                                           taps.data_ptr(), y.data_ptr(), L.stream_handle()))
+    return _from_last(y, ax, x.ndim)
+
+
+_PADTYPES = {"odd": L.PAD_ODD, "even": L.PAD_EVEN, "constant": L.PAD_CONSTANT, None: L.PAD_NONE,
+             "none": L.PAD_NONE}
+
+
+def firfilter2(b: torch.Tensor, x: torch.Tensor, axis: int = -1, padtype: Optional[str] = "odd",
+               padlen: Optional[int] = None, method: str = "pad", irlen: Optional[int] = None,
+               pad_rounding: int = 0) -> torch.Tensor:
+    """Zero-phase FIR along ``axis`` (cuSignal ``firfilter2(b, x, axis=-1, padtype='odd',
+    padlen=None, method='pad', irlen=None)``; filtering_typed.cpp:1226-1302, 1631-1730):
+    reflection padding by ``padlen`` samples (default 3 * len(b)), forward and backward FIR
+    with steady-state initial conditions, crop.  ``irlen`` is ignored by the pad method, as
+    in the reference; ``method='gust'`` is not supported there either.  ``pad_rounding``
+    (``L.PAD_ROUND_*``) rounds odd-reflected pad values as a half / integer input would."""
+    if method == "gust":
+        raise ValueError("firfilter2 gust is not supported by cuSignal 23.08.00")
+    if method != "pad":
+        raise ValueError("firfilter2 method")
+    if padtype not in _PADTYPES:
+        raise ValueError("firfilter2 padtype")
+    b = _real_input(b, "b").contiguous()
+    x = _real_input(x, "x")
+    if b.ndim != 1 or b.numel() < 1:
+        raise ValueError("firfilter2 coefficients")
+    xm, ax = _to_last(x, axis)
+    n = xm.shape[-1]
+    lines = xm.numel() // n if n else 0
+    y = torch.empty_like(xm)
+    L.check(L.lib().zkx_firfilter2_f32(b.data_ptr(), b.numel(), xm.data_ptr(), lines, n, _PADTYPES[padtype],
+                                       int(padlen is not None), int(padlen or 0), int(pad_rounding),
+                                       y.data_ptr(), L.stream_handle()))
+    return _from_last(y, ax, x.ndim)
+
+
+def hilbert(x: torch.Tensor, N: Optional[int] = None, axis: int = -1) -> torch.Tensor:
+    """Analytic signal along ``axis`` (cuSignal ``hilbert(x, N=None, axis=-1)``;
+    filtering_typed.cpp:500-562, 1819-1872): x zero-padded or truncated to N, DFT, bins
+    1..ceil(N/2)-1 doubled, the upper half zeroed, inverse DFT.  complex64 result with N
+    samples along ``axis``."""
+    x = _real_input(x, "x")
+    xm, ax = _to_last(x, axis)
+    n = xm.shape[-1]
+    nfft = n if N is None else int(N)
+    if nfft <= 0:
+        raise ValueError("hilbert N must be positive")
+    lines = int(np.prod(xm.shape[:-1])) if xm.ndim > 1 else 1
+    y = torch.empty(xm.shape[:-1] + (nfft,), dtype=torch.complex64, device=x.device)
+    L.check(L.lib().zkx_hilbert_f32(xm.data_ptr(), lines, n, nfft, y.data_ptr(), L.stream_handle()))
     return _from_last(y, ax, x.ndim)
