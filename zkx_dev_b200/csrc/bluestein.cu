@@ -5,8 +5,8 @@
 //   X[k] = conj(w[k]) * sum_j (x[j] conj(w[j])) w[k - j],   w[m] = exp(i pi m^2 / n),
 //
 // a circular convolution of length M = next pow2(2n - 1) (so n <= 32768) on the library's
-// power-of-two FFTs: pre-multiplication, forward FFT, product with the FFT of the chirp,
-// inverse FFT, post-multiplication.  The inverse DFT runs the same steps on conjugated data.
+// power-of-two transforms: pre-multiplication, then one pass of the range-compression kernel
+// (forward FFT, product with the FFT of the chirp, inverse FFT), post-multiplication.  The inverse DFT runs the same steps on conjugated data.
 // Chirp phases are reduced exactly in integers (m^2 mod 2n) and evaluated in FP64.
 //
 // The same row pipeline with n a power of two and no chirp (M = n, plain FFT) serves Doppler
@@ -33,8 +33,10 @@ __device__ __forceinline__ float2 chirp(long long m, int n)
     return make_float2((float)c, (float)s);
 }
 
-// W[j] = w[j] for j < n; B[m] = w[m] for m < n, B[M - m] = w[m] for 0 < m < n, zero between.
-__global__ void chirp_tables_kernel(int n, int M, float2* __restrict__ B, float2* __restrict__ W)
+// W[j] = w[j] for j < n; h[m] = conj(w[m]) for m < n, h[M - m] = conj(w[m]) for 0 < m < n,
+// zero between.  h is the conjugate of the even convolution kernel b, so the compression
+// spectrum conj(FFT(h)) / M equals FFT(b) / M.
+__global__ void chirp_tables_kernel(int n, int M, float2* __restrict__ h, float2* __restrict__ W)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= M) return;
@@ -45,7 +47,7 @@ __global__ void chirp_tables_kernel(int n, int M, float2* __restrict__ B, float2
     } else if (M - i < n) {
         v = chirp(M - i, n);
     }
-    B[i] = v;
+    h[i] = make_float2(v.x, -v.y);
 }
 
 // a[r][j] = x_r[j] (conjugated when conj_in) * conj(W[j]) for j < n_in, zero up to M.
@@ -66,16 +68,6 @@ __global__ void rows_pre_kernel(const Src src, int row0, int rows, int n_in, int
         }
         a[e] = v;
     }
-}
-
-// a[r][k] *= B[k]
-__global__ void chirp_product_kernel(float2* __restrict__ a, const float2* __restrict__ B, int rows, int log_m)
-{
-    const long long total = (long long)rows << log_m;
-    const int mask = (1 << log_m) - 1;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-         e += (long long)gridDim.x * blockDim.x)
-        a[e] = cmul(a[e], B[e & mask]);
 }
 
 // y[row0 + r][k] = scale * (a[r][k] * conj(W[k])) (conjugated when conj_out), k < n.
@@ -221,7 +213,7 @@ unsigned grid_for(long long elems)
 struct Dft {
     int n = 0, M = 0, log_m = 0;
     bool direct = false;    // n a power of two: plain FFT of length n, no chirp
-    float2* B = nullptr;    // FFT of the chirp, M entries
+    float2* S = nullptr;    // FFT(b) / M in the layout of the compression kernels, M entries
     float2* W = nullptr;    // chirp, n entries (nullptr when direct)
     float2* a = nullptr;    // pass workspace, chunk x M
     int chunk = 0;          // rows per pass
@@ -236,7 +228,8 @@ int prepare(int n, long long rows, cudaStream_t s, StreamWorkspace* ws, Dft* d)
         for (M = 1; M < 2 * n - 1; M <<= 1) {}
     d->M = M;
     d->log_m = ilog2_host(M);
-    const size_t table = d->direct ? 0 : (size_t)M + (((size_t)n + 1) & ~size_t(1));  // a stays 16-byte aligned
+    // S (M) | h (M) | W (n, rounded up to keep a 16-byte aligned) | a
+    const size_t table = d->direct ? 0 : 2 * (size_t)M + (((size_t)n + 1) & ~size_t(1));
     const long long fit = std::max(1LL, (long long)(kPassBytes / ((size_t)M * sizeof(float2))));
     d->chunk = (int)std::max(1LL, std::min(rows, fit));
     ws->stream = s;
@@ -244,21 +237,21 @@ int prepare(int n, long long rows, cudaStream_t s, StreamWorkspace* ws, Dft* d)
     float2* base = static_cast<float2*>(ws->ptr);
     d->a = base + table;
     if (d->direct) return ZKX_SUCCESS;
-    d->B = base;
-    d->W = base + M;
-    chirp_tables_kernel<<<(M + 255) / 256, 256, 0, s>>>(n, M, d->B, d->W);
+    d->S = base;
+    float2* h = base + M;
+    d->W = base + 2 * M;
+    chirp_tables_kernel<<<(M + 255) / 256, 256, 0, s>>>(n, M, h, d->W);
     ZKX_LAUNCHED("chirp_tables_kernel");
-    return launch_fft_rows(d->B, 1, M, 0, d->B, s);
+    return launch_replica_spectrum(h, M, M, 0, ZKX_WINDOW_NONE, nullptr, d->S, s);
 }
 
-// The circular convolution with the chirp (or the plain forward FFT when direct), in place.
+// The circular convolution with the chirp in place -- one pass of the range-compression
+// kernels (forward FFT, product with S, inverse FFT per row) -- or the plain forward FFT
+// when direct.
 int convolve(const Dft& d, int rows, cudaStream_t s)
 {
-    ZKX_TRY(launch_fft_rows(d.a, rows, d.M, 0, d.a, s));
-    if (d.direct) return ZKX_SUCCESS;
-    chirp_product_kernel<<<grid_for((long long)rows << d.log_m), 256, 0, s>>>(d.a, d.B, rows, d.log_m);
-    ZKX_LAUNCHED("chirp_product_kernel");
-    return launch_fft_rows(d.a, rows, d.M, 1, d.a, s);  // scaled by 1/M
+    if (d.direct) return launch_fft_rows(d.a, rows, d.M, 0, d.a, s);
+    return launch_pulse_compression_variant(d.a, rows, d.M, d.M, d.S, d.a, ZKX_COMPRESSION_DEFAULT, s);
 }
 
 // Row DFTs of length n over `rows` rows of src (first n_in samples, zero beyond), written

@@ -11,7 +11,8 @@
 //   f[i] = sum_k b[k] E(i - k),   E(i < 0) = E(0)
 //   y[m] = sum_k b[k] F(edge + m + k),   F(i >= ne - 1) = f[ne - 1],   ne = n + 2 edge.
 //
-// One CTA produces 4096 outputs of one line in a single HBM pass: the extended input
+// One CTA produces 16 (256 s - nbp / 16) outputs of one line (s sweeps, nbp = nb rounded up to
+// 16) in a single HBM pass: the extended input
 // window (with both halos) is built in shared memory straight from x, the forward pass
 // writes the f window next to it, the backward pass reads it with the taps reversed.
 // Both passes use the blocked register FIR of the causal filter (16 consecutive outputs
@@ -35,7 +36,6 @@ namespace {
 
 constexpr int kZpThreads = 256;
 constexpr int kZpPer = 16;
-constexpr int kZpBlock = kZpThreads * kZpPer;  // outputs per CTA
 constexpr int kMaxZpTaps = 4096;
 
 __host__ __device__ __forceinline__ int zp_word(int block) { return 20 * block; }  // 16 samples + 4 pad words
@@ -112,16 +112,19 @@ __device__ __forceinline__ void fir16(const float* __restrict__ taps, const floa
     }
 }
 
-// Shared layout (floats): taps[nbp] | reversed taps[nbp] | E window (fb + chunks blocks)
-// | F window (fb blocks), fb = 256 + chunks.  E block j holds E(o0 - nbp + 1 + 16 j + s),
-// F block j holds F(o0 + 16 j + s), o0 = edge + 4096 * blockIdx.x.
-__global__ void __launch_bounds__(kZpThreads)
-firfilter2_kernel(const float* __restrict__ b, int nb, int nbp, const float* __restrict__ x, int lines, int n,
-                  int edge, int padtype, int rounding, float* __restrict__ y)
+// The F window is fb = 256 * sweeps blocks of 16, one block per thread per sweep, and the
+// CTA's outputs are the tb = fb - nbp / 16 blocks whose backward taps it covers, so both
+// passes keep every thread busy.  Shared layout (floats): taps[nbp] | reversed taps[nbp] |
+// E window (fb + nbp / 16 blocks) | F window (fb blocks).  E block j holds
+// E(o0 - nbp + 1 + 16 j + s), F block j holds F(o0 + 16 j + s), o0 = edge + 16 tb blockIdx.x.
+__global__ void __launch_bounds__(kZpThreads, 4)
+firfilter2_kernel(const float* __restrict__ b, int nb, int nbp, int sweeps, const float* __restrict__ x,
+                  int lines, int n, int edge, int padtype, int rounding, float* __restrict__ y)
 {
     extern __shared__ __align__(16) float zsm[];
     const int chunks = nbp >> 4;
-    const int fb = kZpBlock / 16 + chunks;
+    const int fb = kZpThreads * sweeps;
+    const int tb = fb - chunks;
     float* taps = zsm;
     float* rtaps = zsm + nbp;
     float* es = rtaps + nbp;
@@ -135,14 +138,15 @@ firfilter2_kernel(const float* __restrict__ b, int nb, int nbp, const float* __r
     }
     for (int line = blockIdx.y; line < lines; line += gridDim.y) {
         const float* xl = x + (size_t)line * n;
-        const long long o0 = edge + (long long)blockIdx.x * kZpBlock;
+        const long long o0 = edge + (long long)blockIdx.x * 16 * tb;
         const int espan = 16 * (fb + chunks);
         for (int j = threadIdx.x; j < espan; j += kZpThreads) {
             const long long i = o0 - hist + j;
             es[zp_word(j >> 4) + (j & 15)] = i < ne ? extended_sample(xl, n, edge, padtype, rounding, i) : 0.f;
         }
-        if (threadIdx.x < 32) {
-            // f[ne - 1], the value the backward pass extends the forward output with
+        if (threadIdx.x < 32 && o0 + 16LL * fb >= ne) {
+            // f[ne - 1], the value the backward pass extends the forward output with (only
+            // the CTAs whose F window reaches the end of the line read it)
             float v = 0.f;
             for (int k = threadIdx.x; k < nb; k += 32)
                 v = fmaf(b[k], extended_sample(xl, n, edge, padtype, rounding, ne - 1 - k), v);
@@ -154,25 +158,27 @@ firfilter2_kernel(const float* __restrict__ b, int nb, int nbp, const float* __r
         float acc[kZpPer];
         for (int ob = threadIdx.x; ob < fb; ob += kZpThreads) {
             fir16(taps, es, ob, chunks, acc);
+            // window positions at or past ne - 1 hold f[ne - 1]
+            const long long past = ne - 1 - o0 - 16LL * ob;
+            const int first = past < 0 ? 0 : (past > kZpPer ? kZpPer : (int)past);
 #pragma unroll
-            for (int q = 0; q < kZpPer; ++q) {
-                const long long i = o0 + 16LL * ob + q;
-                fs[zp_word(ob) + q] = i >= ne - 1 ? f_last : acc[q];
-            }
+            for (int q = 0; q < kZpPer; ++q) fs[zp_word(ob) + q] = q >= first ? f_last : acc[q];
         }
         __syncthreads();
-        fir16(rtaps, fs, threadIdx.x, chunks, acc);
-        const long long m0 = (long long)blockIdx.x * kZpBlock + kZpPer * threadIdx.x;
         float* yl = y + (size_t)line * n;
-        if (m0 + kZpPer <= n && (reinterpret_cast<uintptr_t>(yl + m0) & 15) == 0) {
-            float4* yp = reinterpret_cast<float4*>(yl + m0);
+        for (int ob = threadIdx.x; ob < tb; ob += kZpThreads) {
+            fir16(rtaps, fs, ob, chunks, acc);
+            const long long m0 = (long long)blockIdx.x * 16 * tb + 16LL * ob;
+            if (m0 + kZpPer <= n && (reinterpret_cast<uintptr_t>(yl + m0) & 15) == 0) {
+                float4* yp = reinterpret_cast<float4*>(yl + m0);
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-                __stcs(&yp[u], make_float4(acc[4 * u], acc[4 * u + 1], acc[4 * u + 2], acc[4 * u + 3]));
-        } else {
+                for (int u = 0; u < 4; ++u)
+                    __stcs(&yp[u], make_float4(acc[4 * u], acc[4 * u + 1], acc[4 * u + 2], acc[4 * u + 3]));
+            } else {
 #pragma unroll
-            for (int q = 0; q < kZpPer; ++q)
-                if (m0 + q < n) yl[m0 + q] = acc[q];
+                for (int q = 0; q < kZpPer; ++q)
+                    if (m0 + q < n) yl[m0 + q] = acc[q];
+            }
         }
         __syncthreads();  // the windows are rebuilt for the next line
     }
@@ -271,11 +277,15 @@ int launch_firfilter2(const float* b, int nb, const float* x, int lines, int n, 
 {
     if (nb > kMaxZpTaps) return fail(ZKX_UNSUPPORTED_OPERATION, "firfilter2: more than 4096 coefficients");
     const int nbp = (nb + 15) & ~15;
-    const int chunks = nbp / 16, fb = kZpBlock / 16 + chunks;
+    const int chunks = nbp / 16;
+    const int sweeps = (chunks + 64 + kZpThreads - 1) / kZpThreads;  // at least 64 output blocks per CTA
+    const int fb = kZpThreads * sweeps, tb = fb - chunks;
     const size_t smem = (2 * (size_t)nbp + zp_word(fb + chunks) + zp_word(fb)) * sizeof(float);
     ZKX_CUDA(cudaFuncSetAttribute(firfilter2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const dim3 grid((unsigned)((n + kZpBlock - 1) / kZpBlock), (unsigned)(lines < 65535 ? lines : 65535));
-    firfilter2_kernel<<<grid, kZpThreads, smem, stream>>>(b, nb, nbp, x, lines, n, edge, padtype, rounding, y);
+    const long long per_cta = 16LL * tb;
+    const dim3 grid((unsigned)((n + per_cta - 1) / per_cta), (unsigned)(lines < 65535 ? lines : 65535));
+    firfilter2_kernel<<<grid, kZpThreads, smem, stream>>>(b, nb, nbp, sweeps, x, lines, n, edge, padtype, rounding,
+                                                          y);
     ZKX_LAUNCHED("firfilter2_kernel");
     return ZKX_SUCCESS;
 }
