@@ -7,8 +7,8 @@
 // max_inflight batches queued on the GPU) and its workspace fits the HBM budget.  A
 // batch is a three-stage pipeline over the server's streams:
 //
-//   copy-in stream   workspace from the stream-ordered pool; host-resident CPIs copied
-//                    into it (device-resident CPIs are read in place)
+//   copy-in stream   host-resident CPIs copied into the batch's workspace (device-resident
+//                    CPIs are read in place)
 //   compute stream   zkx_rd_execute_batch kernels, one launch per stage for the whole
 //                    batch (range compression reads the CPIs through a pointer table)
 //   copy-out stream  the requested outputs copied to each request's buffers, the
@@ -17,9 +17,14 @@
 // so while one batch computes, the next copies in and the previous copies out, and the
 // kernels of consecutive batches stay in order on one compute stream (a producer's
 // output is still in L2 when its consumer runs).  The callback returns the workspace
-// bytes to the budget and wakes the worker, which admits more requests without waiting
-// for the rest of the device work: requests that arrive while others are on the GPU
-// join as soon as slots and memory free up.
+// to the server's idle list and its bytes to the budget and wakes the worker, which admits
+// more requests without waiting for the rest of the device work: requests that arrive
+// while others are on the GPU join as soon as slots and memory free up.
+//
+// Workspaces are device blocks the server keeps: a batch takes an idle block of its size
+// (up to 1.5x) or a new one, and gives it back from its completion callback, when every
+// copy and kernel that used it has finished.  After the first batches of each shape no
+// allocation happens at all, and no stream ever waits for another batch's memory.
 //
 // Plans (replica spectrum and Doppler window, resident) are cached per (pulses,
 // samples, replica length, waveform id) for the server's lifetime; a plan is built on
@@ -31,6 +36,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <iterator>
 #include <map>
 #include <mutex>
 #include <string>
@@ -108,7 +114,8 @@ struct zkx_rd_server_s {
     std::vector<cudaStream_t> streams;  // compute streams
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
     std::vector<cudaEvent_t> free_events;  // reusable; returned by completion callbacks
-    cudaMemPool_t pool = nullptr;
+    std::multimap<size_t, char*> idle;  // workspace blocks not in use, by size
+    size_t held = 0;                    // bytes of every workspace block, in use or idle
     size_t budget = 0, in_use = 0, peak = 0, plan_bytes = 0;
 
     std::mutex mu;
@@ -134,7 +141,8 @@ namespace {
 struct Batch {
     zkx_rd_server_s* s = nullptr;
     std::vector<Request*> reqs;
-    size_t bytes = 0;
+    char* ws = nullptr;    // workspace block
+    size_t bytes = 0;      // its size
     bool with_rd = false;  // some request of the batch wants the complex map
     int staged = 0;        // host-resident CPIs copied into the workspace
     cudaEvent_t in = nullptr, done = nullptr;
@@ -167,6 +175,7 @@ void CUDART_CB batch_done(void* arg)
     {
         std::lock_guard<std::mutex> lk(s->mu);
         finish_requests(s, b->reqs, ZKX_SUCCESS, std::string(), now);
+        s->idle.emplace(b->bytes, b->ws);
         s->in_use -= b->bytes;
         --s->inflight;
         s->free_events.push_back(b->in);
@@ -218,12 +227,7 @@ int issue_batch(zkx_rd_server_s* s, const PlanEntry& pe, Batch* b, const Layout&
     const int P = head.r.num_pulses, N = head.r.samples_per_pulse;
     const size_t cube = (size_t)P * N, map = (size_t)pe.doppler_bins * pe.range_bins;
     const int count = (int)b->reqs.size();
-    char* ws = nullptr;
-    ZKX_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), l.total, s->pool, s->copy_in));
-    auto release = [&](int rc) {
-        cudaFreeAsync(ws, s->copy_in);
-        return rc;
-    };
+    char* ws = b->ws;
     const void* table[kMaxRowTable];
     float2* staged = reinterpret_cast<float2*>(ws + l.x);
     int slot = 0;
@@ -235,32 +239,23 @@ int issue_batch(zkx_rd_server_s* s, const PlanEntry& pe, Batch* b, const Layout&
         }
         float2* dst = staged + (size_t)slot++ * cube;
         cudaError_t e = cudaMemcpyAsync(dst, q.r.x, cube * sizeof(float2), cudaMemcpyDefault, s->copy_in);
-        if (e != cudaSuccess) return release(cuda_status(e, "serving input copy"));
+        if (e != cudaSuccess) return cuda_status(e, "serving input copy");
         table[i] = dst;
     }
     cudaError_t e = cudaEventRecord(b->in, s->copy_in);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(compute, b->in, 0);
-    if (e != cudaSuccess) return release(cuda_status(e, "serving pipeline event"));
+    if (e != cudaSuccess) return cuda_status(e, "serving pipeline event");
     float2* rd = b->with_rd ? reinterpret_cast<float2*>(ws + l.rd) : nullptr;
     float* power = reinterpret_cast<float*>(ws + l.power);
     float* thr = reinterpret_cast<float*>(ws + l.threshold);
     uint8_t* det = reinterpret_cast<uint8_t*>(ws + l.detections);
     float* cum = s->d.cfar_mode == ZKX_CFAR_COMPAT ? reinterpret_cast<float*>(ws + l.cumulative) : nullptr;
-    // from here on the workspace is in use on the compute stream: a failure frees it
-    // after that stream's queued work
-    auto release_after_compute = [&](int rc) {
-        if (cudaEventRecord(b->done, compute) != cudaSuccess ||
-            cudaStreamWaitEvent(s->copy_in, b->done, 0) != cudaSuccess)
-            cudaStreamSynchronize(compute);
-        cudaFreeAsync(ws, s->copy_in);
-        return rc;
-    };
     int rc = rd_execute_batch_ws(pe.plan, nullptr, count, ws + l.compressed, rd, power, thr, det, cum,
                                  compute, table);
-    if (rc != ZKX_SUCCESS) return release_after_compute(rc);
+    if (rc != ZKX_SUCCESS) return rc;
     e = cudaEventRecord(b->done, compute);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s->copy_out, b->done, 0);
-    if (e != cudaSuccess) return release_after_compute(cuda_status(e, "serving pipeline event"));
+    if (e != cudaSuccess) return cuda_status(e, "serving pipeline event");
     for (int i = 0; i < count; ++i) {
         const zkx_rd_request& q = b->reqs[i]->r;
         e = cudaMemcpyAsync(q.detections, det + i * map, map, cudaMemcpyDefault, s->copy_out);
@@ -270,13 +265,45 @@ int issue_batch(zkx_rd_server_s* s, const PlanEntry& pe, Batch* b, const Layout&
             e = cudaMemcpyAsync(q.power, power + i * map, map * 4, cudaMemcpyDefault, s->copy_out);
         if (e == cudaSuccess && q.rd)
             e = cudaMemcpyAsync(q.rd, rd + i * map, map * 8, cudaMemcpyDefault, s->copy_out);
-        if (e != cudaSuccess) {
-            cudaFreeAsync(ws, s->copy_out);
-            return cuda_status(e, "serving output copy");
-        }
+        if (e != cudaSuccess) return cuda_status(e, "serving output copy");
     }
-    ZKX_CUDA(cudaFreeAsync(ws, s->copy_out));
     ZKX_CUDA(cudaLaunchHostFunc(s->copy_out, batch_done, b));
+    return ZKX_SUCCESS;
+}
+
+// A workspace block of at least `need` bytes for a batch admitted under the budget; called
+// by the worker with the lock held, which it drops around allocation and release calls.
+// An idle block of up to 1.5x the size is reused; otherwise idle blocks are released
+// (largest first) until a new block fits within the budget next to the blocks in use.
+int acquire_block(zkx_rd_server_s* s, std::unique_lock<std::mutex>& lk, size_t need, char** ws,
+                  size_t* bytes)
+{
+    auto it = s->idle.lower_bound(need);
+    if (it != s->idle.end() && it->first <= need + need / 2) {
+        *ws = it->second;
+        *bytes = it->first;
+        s->idle.erase(it);
+        return ZKX_SUCCESS;
+    }
+    std::vector<char*> release;
+    while (s->held + need + s->plan_bytes > s->budget && !s->idle.empty()) {
+        auto last = std::prev(s->idle.end());
+        s->held -= last->first;
+        release.push_back(last->second);
+        s->idle.erase(last);
+    }
+    s->held += need;
+    lk.unlock();
+    for (char* p : release) cudaFree(p);  // waits for the device; completions need the lock
+    char* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, need);
+    lk.lock();
+    if (e != cudaSuccess) {
+        s->held -= need;
+        return cuda_status(e, "serving workspace");
+    }
+    *ws = p;
+    *bytes = need;
     return ZKX_SUCCESS;
 }
 
@@ -368,16 +395,26 @@ void worker_main(zkx_rd_server_s* s)
             continue;
         }
         for (Request* q : group) s->pending.erase(std::find(s->pending.begin(), s->pending.end(), q));
-        s->in_use += l.total;
+        char* block = nullptr;
+        size_t block_bytes = 0;
+        ++s->inflight;  // holds the slot while the lock may be dropped
+        int arc = acquire_block(s, lk, l.total, &block, &block_bytes);
+        if (arc != ZKX_SUCCESS) {
+            --s->inflight;
+            finish_requests(s, group, arc, std::string(zkx_last_error()), Clock::now());
+            s->done_cv.notify_all();
+            continue;
+        }
+        s->in_use += block_bytes;
         s->peak = std::max(s->peak, s->in_use);
-        ++s->inflight;
         ++s->next_stream;
         ++s->batches;
         s->batched_cpis += group.size();
         Batch* b = new Batch;
         b->s = s;
         b->reqs = group;
-        b->bytes = l.total;
+        b->ws = block;
+        b->bytes = block_bytes;
         b->with_rd = with_rd;
         b->staged = staged;
         int rc = take_event(s, &b->in);
@@ -385,9 +422,16 @@ void worker_main(zkx_rd_server_s* s)
         lk.unlock();
         if (rc == ZKX_SUCCESS) rc = issue_batch(s, pe, b, l, stream);
         const std::string msg = rc == ZKX_SUCCESS ? std::string() : std::string(zkx_last_error());
+        if (rc != ZKX_SUCCESS) {
+            // work already queued may still read the block: let it drain before reuse
+            cudaStreamSynchronize(s->copy_in);
+            cudaStreamSynchronize(stream);
+            cudaStreamSynchronize(s->copy_out);
+        }
         lk.lock();
         if (rc != ZKX_SUCCESS) {
             finish_requests(s, b->reqs, rc, msg, Clock::now());
+            s->idle.emplace(b->bytes, b->ws);
             s->in_use -= b->bytes;
             --s->inflight;
             if (b->in) s->free_events.push_back(b->in);
@@ -441,7 +485,6 @@ extern "C" int zkx_rd_server_create(const zkx_rd_server_desc* desc, zkx_rd_serve
         for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
         if (s->copy_in) cudaStreamDestroy(s->copy_in);
         if (s->copy_out) cudaStreamDestroy(s->copy_out);
-        if (s->pool) cudaMemPoolDestroy(s->pool);
         delete s;
         return rc;
     };
@@ -451,15 +494,6 @@ extern "C" int zkx_rd_server_create(const zkx_rd_server_desc* desc, zkx_rd_serve
     if (e != cudaSuccess) return cleanup(cuda_status(e, "rd_server_create"));
     s->budget = (size_t)(d.hbm_fraction * (double)free_bytes);
     if (d.budget_bytes) s->budget = std::min(s->budget, d.budget_bytes);
-    cudaMemPoolProps props{};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = s->device;
-    e = cudaMemPoolCreate(&s->pool, &props);
-    if (e != cudaSuccess) return cleanup(cuda_status(e, "rd_server_create: memory pool"));
-    uint64_t keep = UINT64_MAX;  // keep freed workspaces in the pool for the next batches
-    e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    if (e != cudaSuccess) return cleanup(cuda_status(e, "rd_server_create: memory pool"));
     for (int i = 0; i < d.streams; ++i) {
         cudaStream_t st;
         e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
@@ -494,7 +528,7 @@ extern "C" int zkx_rd_server_destroy(zkx_rd_server s)
         cudaEventDestroy(kv.second.ready);
         zkx_rd_plan_destroy(kv.second.plan);
     }
-    cudaMemPoolDestroy(s->pool);
+    for (auto& kv : s->idle) cudaFree(kv.second);
     for (auto& kv : s->requests) delete kv.second;
     delete s;
     return ZKX_SUCCESS;
