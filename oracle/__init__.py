@@ -47,6 +47,15 @@ def build_reference(ref_root: str = "/root/reference") -> bool:
     return True
 
 
+def build_probes(ref_root: str = "/root/reference") -> bool:
+    """Compile the reference's own operator probes against include/ and libzkx_rd.so
+    (test infrastructure for the drop-in check) when the reference checkout is present."""
+    if not os.path.isdir(os.path.join(ref_root, "ZKX", "test_all")):
+        return False
+    subprocess.run(["make", "-s", "-j8", "-C", _HERE, "probes", f"REF_ROOT={ref_root}"], check=True)
+    return True
+
+
 _lib_cache: dict = {}
 
 
