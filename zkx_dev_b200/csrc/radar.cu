@@ -146,6 +146,13 @@ pulse_compression_persistent_kernel(const Src src, int pulses, int samples,
             return;
         }
         phase ^= 1u;
+        // the next pulse can only be copied into shared memory once this one's exchanges
+        // are done; pull it into L2 now so that copy reads L2 instead of HBM
+        if (t == 0 && pulse + (int)gridDim.x < pulses) {
+            const char* from = reinterpret_cast<const char*>(src.row(pulse + gridDim.x));
+            for (uint32_t off = 0; off < bytes; off += kChunk)
+                bulk_prefetch_l2(from + off, bytes - off < kChunk ? bytes - off : kChunk);
+        }
         float2 v[PL::E];
 #pragma unroll
         for (int r = 0; r < PL::E; ++r) {

@@ -77,6 +77,13 @@ __device__ __forceinline__ void bulk_load_1d(void* dst, const void* src, uint32_
 
 // Orders this thread's earlier generic-proxy shared-memory accesses before later
 // async-proxy (bulk copy) writes to the same memory.
+// Asynchronous prefetch of [src, src + bytes) from global memory into L2 (no completion
+// signal; src 16-byte aligned, bytes a multiple of 16).
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void fence_proxy_async_smem()
 {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
