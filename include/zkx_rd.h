@@ -284,6 +284,16 @@ ZKX_API int zkx_firfilter2_f32(const float* b, int nb, const float* x, int lines
  * 1813-1872; device computation filtering_typed.cu:327-352). */
 ZKX_API int zkx_hilbert_f32(const float* x, int lines, int n, int nfft, void* y, zkx_stream_t stream);
 
+/* FIR evaluation method of zkx_fir_ex_f32. */
+enum {
+    ZKX_FIR_AUTO = 0,    /* by tap count */
+    ZKX_FIR_DIRECT = 1,  /* direct sums, 16 outputs per thread from shared memory */
+    ZKX_FIR_FFT = 2      /* overlap-save convolution, two lines per complex transform (<= 4096 taps) */
+};
+/* zkx_fir_f32 with an explicit evaluation method (same results within FP32 rounding). */
+ZKX_API int zkx_fir_ex_f32(const float* b, int nb, const float* x, int lines, int n, const float* zi,
+                           float* y, float* zf, int method, zkx_stream_t stream);
+
 /* Output length of upfirdn: floor(((n-1)*up + nh - 1) / down) + 1
  * (src/operators/filtering/filtering_typed.cpp:1091-1098). */
 ZKX_API long long zkx_upfirdn_length(int n, int nh, int up, int down);

@@ -22,6 +22,7 @@ WINDOW_NONE, WINDOW_HANN, WINDOW_HAMMING, WINDOW_EXPLICIT_FP32, WINDOW_EXPLICIT_
 CFAR_ACCURATE, CFAR_COMPAT = 0, 1
 PRECISION_FP32, PRECISION_TC_F16, PRECISION_TC_BF16 = 0, 1, 2
 PAD_ODD, PAD_EVEN, PAD_CONSTANT, PAD_NONE = range(4)
+FIR_AUTO, FIR_DIRECT, FIR_FFT = range(3)
 PAD_ROUND_F32, PAD_ROUND_F16, PAD_ROUND_I8, PAD_ROUND_I16, PAD_ROUND_I32 = range(5)
 
 # Every symbol the header declares, with its ctypes signature.
@@ -93,6 +94,7 @@ SIGNATURES = {
     "zkx_cfar_reference_count": (_I, [_I, _I, _I, _I, _I]),
     "zkx_ca_cfar_f32": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _D, _I, _P, _P, _P]),
     "zkx_fir_f32": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P]),
+    "zkx_fir_ex_f32": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _I, _P]),
     "zkx_firfilter2_f32": (_I, [_P, _I, _P, _I, _I, _I, _I, _I, _I, _P, _P]),
     "zkx_hilbert_f32": (_I, [_P, _I, _I, _I, _P, _P]),
     "zkx_upfirdn_length": (ctypes.c_longlong, [_I, _I, _I, _I]),

@@ -235,6 +235,19 @@ extern "C" int zkx_fir_f32(const float* b, int nb, const float* x, int lines, in
     return launch_fir(b, nb, x, lines, n, zi, y, zi ? zf : nullptr, stream);
 }
 
+extern "C" int zkx_fir_ex_f32(const float* b, int nb, const float* x, int lines, int n, const float* zi,
+                              float* y, float* zf, int method, zkx_stream_t stream)
+{
+    if (method < ZKX_FIR_AUTO || method > ZKX_FIR_FFT) return fail(ZKX_INVALID_ARGUMENT, "firfilter: unknown method");
+    if (nb < 1) return fail(ZKX_INVALID_ARGUMENT, "firfilter coefficients");
+    if (lines < 1 || n < 1 || (long long)lines * n > INT_MAX)
+        return fail(ZKX_INVALID_SHAPE, "firfilter input shape");
+    if (!b || !x || !y || (zi && nb > 1 && !zf)) return fail(ZKX_INVALID_ARGUMENT, "firfilter: null pointer");
+    if (method == ZKX_FIR_FFT && nb > 4096) return fail(ZKX_UNSUPPORTED_OPERATION, "firfilter: FFT method takes at most 4096 taps");
+    ZKX_TRY(ensure_device_ready());
+    return launch_fir(b, nb, x, lines, n, zi, y, zi ? zf : nullptr, stream, method);
+}
+
 extern "C" long long zkx_upfirdn_length(int n, int nh, int up, int down)
 {
     if (nh < 1 || up < 1 || down < 1 || n < 0) return -1;

@@ -1,0 +1,113 @@
+// Long causal FIR filters as overlap-save convolutions on the library's Stockham transforms.
+//
+// Two real lines a, b form one complex signal z = x_a + i x_b.  The taps are real, so
+// IFFT(FFT(z) . FFT(h)) carries the two convolutions in its real and imaginary parts.  A
+// block of N samples (N = 4096 for up to 512 taps, 8192 / 16384 for longer filters) yields
+// its last N - (nb - 1) outputs, the ones whose window lies inside the block; block j
+// starts nb - 1 samples before its first output, so the blocks tile the line with zero
+// extension before sample 0 (the causal definition of filtering_typed.cpp:1545-1590).
+// Each block is one CTA-resident transform pair: load, forward FFT, product with the tap
+// spectrum (scaled by 1/N), inverse FFT, store -- one HBM pass, about 2 x 5 log2 N flops per
+// complex sample instead of 2 nb per real output.
+#include "fft_core.cuh"
+#include "zkx_internal.h"
+
+namespace zkx {
+namespace {
+
+// row[k] = (k < nb ? b[k] / N : 0) + 0i, the scaled, zero-padded taps before their FFT
+__global__ void fir_taps_row_kernel(const float* __restrict__ b, int nb, int N, float2* __restrict__ row)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < N) row[k] = make_float2(k < nb ? b[k] / (float)N : 0.f, 0.f);
+}
+
+template <int N, int G>
+__global__ void __launch_bounds__(G * FftPlan<N, elems_for(N)>::T)
+fir_fft_kernel(const float* __restrict__ x, int lines, int n, int nb, const float2* __restrict__ H,
+               const float* __restrict__ zi, float* __restrict__ y, const float2* __restrict__ tw)
+{
+    using PL = FftPlan<N, elems_for(N)>;
+    extern __shared__ float2 sm[];
+    const int g = threadIdx.x / PL::T;
+    const int t = threadIdx.x - g * PL::T;
+    float2* smg = sm + g * PL::smem_elems();
+    const int hist = nb - 1;
+    const int step = N - hist;                         // outputs per block
+    const long long block = (long long)blockIdx.x * G + g;
+    const long long out0 = block * step;               // first output of the block
+    const long long s0 = out0 - hist;                  // first input sample of the block
+    const int la = 2 * blockIdx.y, lb = la + 1;
+    const bool has_b = lb < lines;
+    const bool active = out0 < n;
+    const float* xa = x + (size_t)la * n;
+    const float* xb = x + (size_t)(has_b ? lb : la) * n;
+    float2 v[PL::E];
+#pragma unroll
+    for (int r = 0; r < PL::E; ++r) {
+        const long long s = s0 + t + PL::T * r;
+        const bool in = active && s >= 0 && s < n;
+        v[r] = make_float2(in ? __ldcs(&xa[s]) : 0.f, (in && has_b) ? __ldcs(&xb[s]) : 0.f);
+    }
+    fft_block<PL, -1, 1>(v, smg, t, tw);
+#pragma unroll
+    for (int r = 0; r < PL::E; ++r) v[r] = cmul(v[r], __ldg(&H[t + PL::T * r]));
+    if constexpr (PL::PASSES > 1) __syncthreads();
+    fft_block<PL, 1, 1>(v, smg, t, tw);
+    if (!active) return;
+    float* ya = y + (size_t)la * n;
+    float* yb = y + (size_t)lb * n;
+#pragma unroll
+    for (int r = 0; r < PL::E; ++r) {
+        const int e = t + PL::T * r;
+        const long long o = s0 + e;
+        if (e >= hist && o < n) {
+            float va = v[r].x, vb = v[r].y;
+            if (zi && o < hist) {
+                va += zi[(size_t)la * hist + o];
+                if (has_b) vb += zi[(size_t)lb * hist + o];
+            }
+            ya[o] = va;  // stays in L2 for the next stage
+            if (has_b) yb[o] = vb;
+        }
+    }
+}
+
+template <int N>
+int fir_fft_impl(const float* b, int nb, const float* x, int lines, int n, const float* zi, float* y,
+                 cudaStream_t s)
+{
+    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
+    using PL = FftPlan<N, elems_for(N)>;
+    StreamWorkspace ws;
+    ws.stream = s;
+    ZKX_TRY(stream_workspace((size_t)N * sizeof(float2), s, &ws.ptr));
+    float2* H = static_cast<float2*>(ws.ptr);
+    fir_taps_row_kernel<<<(N + 255) / 256, 256, 0, s>>>(b, nb, N, H);
+    ZKX_LAUNCHED("fir_taps_row_kernel");
+    ZKX_TRY(launch_fft_rows(H, 1, N, 0, H, s));
+    constexpr int G = rows_per_cta(N);
+    const size_t smem = (size_t)G * PL::smem_elems() * sizeof(float2);
+    auto k = fir_fft_kernel<N, G>;
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long long step = N - (nb - 1);
+    const long long blocks = (n + step - 1) / step;
+    const dim3 grid((unsigned)((blocks + G - 1) / G), (unsigned)((lines + 1) / 2));
+    k<<<grid, G * PL::T, smem, s>>>(x, lines, n, nb, H, zi, y, twiddle_table());
+    ZKX_LAUNCHED("fir_fft_kernel");
+    return ZKX_SUCCESS;
+}
+
+}  // namespace
+
+int launch_fir_fft(const float* b, int nb, const float* x, int lines, int n, const float* zi, float* y,
+                   cudaStream_t stream)
+{
+    if ((lines + 1) / 2 > 65535) return fail(ZKX_UNSUPPORTED_OPERATION, "firfilter: more than 131070 lines");
+    if (nb <= 512) return fir_fft_impl<4096>(b, nb, x, lines, n, zi, y, stream);
+    if (nb <= 1024) return fir_fft_impl<8192>(b, nb, x, lines, n, zi, y, stream);
+    if (nb <= 4096) return fir_fft_impl<16384>(b, nb, x, lines, n, zi, y, stream);
+    return fail(ZKX_UNSUPPORTED_OPERATION, "firfilter: more than 4096 taps");
+}
+
+}  // namespace zkx

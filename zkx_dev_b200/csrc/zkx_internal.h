@@ -114,8 +114,12 @@ int launch_ca_cfar_compat(const float* x, int rank, int rows, int columns, int g
                           int guard_columns, int reference_rows, int reference_columns,
                           float alpha, int reference_count, float* cumulative, float* threshold,
                           uint8_t* detections, cudaStream_t stream);
+// method: ZKX_FIR_AUTO (by tap count), ZKX_FIR_DIRECT (register-blocked direct sums) or
+// ZKX_FIR_FFT (overlap-save on the Stockham transforms, firfft.cu; up to 4096 taps).
 int launch_fir(const float* b, int nb, const float* x, int lines, int n, const float* zi,
-               float* y, float* zf, cudaStream_t stream);
+               float* y, float* zf, cudaStream_t stream, int method = ZKX_FIR_AUTO);
+int launch_fir_fft(const float* b, int nb, const float* x, int lines, int n, const float* zi, float* y,
+                   cudaStream_t stream);
 // zkx_rd_execute_batch with an explicit compat-mode integral-image workspace
 // (nd * nr floats; NULL = the plan's own), for callers that run one plan on several
 // streams at once.  With a non-NULL `table` (batch <= kMaxRowTable entries) CPI b is

@@ -41,10 +41,16 @@ def _from_last(y: torch.Tensor, ax: int, nd: int) -> torch.Tensor:
     return y.movedim(-1, ax).contiguous() if ax != nd - 1 else y
 
 
+_FIR_METHODS = {"auto": L.FIR_AUTO, "direct": L.FIR_DIRECT, "fft": L.FIR_FFT}
+
+
 def firfilter(b: torch.Tensor, x: torch.Tensor, axis: int = -1,
-              zi: Optional[torch.Tensor] = None):
+              zi: Optional[torch.Tensor] = None, method: str = "auto"):
     """Causal FIR y = b * x along ``axis`` with the output length of x; with ``zi``
-    returns (y, zf)."""
+    returns (y, zf).  ``method``: "direct" sums, "fft" overlap-save convolution (two lines
+    per complex transform, up to 4096 taps), or "auto" (by tap count)."""
+    if method not in _FIR_METHODS:
+        raise ValueError("firfilter method")
     b = _real_input(b, "b").contiguous()
     x = _real_input(x, "x")
     if b.ndim != 1 or b.numel() < 1:
@@ -61,8 +67,8 @@ def firfilter(b: torch.Tensor, x: torch.Tensor, axis: int = -1,
         if zim.shape[-1] != b.numel() - 1 or zim.numel() != lines * (b.numel() - 1):
             raise ValueError("firfilter zi broadcast shape")
         zf = torch.empty_like(zim)
-    L.check(L.lib().zkx_fir_f32(b.data_ptr(), b.numel(), xm.data_ptr(), lines, n, L.ptr(zim),
-                                y.data_ptr(), L.ptr(zf), L.stream_handle()))
+    L.check(L.lib().zkx_fir_ex_f32(b.data_ptr(), b.numel(), xm.data_ptr(), lines, n, L.ptr(zim),
+                                   y.data_ptr(), L.ptr(zf), _FIR_METHODS[method], L.stream_handle()))
     y = _from_last(y, ax, x.ndim)
     if zi is None:
         return y
