@@ -81,6 +81,9 @@ struct Request {
 };
 
 constexpr size_t kAlign = 256;
+// Cells per fused batch (two 1024 x 16384 CPIs): small CPIs batch up to max_batch, large ones
+// run alone.
+constexpr long long kMaxBatchCells = 1LL << 25;
 size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 
 // Workspace of one batch of `count` CPIs [P, N] (range nfft N, Doppler nfft P), of which
@@ -271,15 +274,29 @@ int issue_batch(zkx_rd_server_s* s, const PlanEntry& pe, Batch* b, const Layout&
     return ZKX_SUCCESS;
 }
 
-// A workspace block of at least `need` bytes for a batch admitted under the budget; called
+// A workspace block of at least `need_bytes` for a batch admitted under the budget; called
 // by the worker with the lock held, which it drops around allocation and release calls.
-// An idle block of up to 1.5x the size is reused; otherwise idle blocks are released
-// (largest first) until a new block fits within the budget next to the blocks in use.
-int acquire_block(zkx_rd_server_s* s, std::unique_lock<std::mutex>& lk, size_t need, char** ws,
+// An idle block of up to twice the size is reused; otherwise idle blocks are released
+// (largest first) until a new block of the size class fits within the budget next to the
+// blocks in use.
+// Block sizes are rounded up to classes 2^k * {1, 1.25, 1.5, 1.75} (at least 1 MB), so that the
+// varying batch compositions of a request stream keep reusing a few blocks instead of
+// allocating new ones (an allocation can stall the device).
+size_t size_class(size_t need)
+{
+    size_t base = size_t(1) << 20;
+    while (base * 2 <= need) base *= 2;
+    for (size_t q = 4; q <= 8; ++q)
+        if (base / 4 * q >= need) return base / 4 * q;
+    return base * 2;
+}
+
+int acquire_block(zkx_rd_server_s* s, std::unique_lock<std::mutex>& lk, size_t need_bytes, char** ws,
                   size_t* bytes)
 {
-    auto it = s->idle.lower_bound(need);
-    if (it != s->idle.end() && it->first <= need + need / 2) {
+    const size_t need = size_class(need_bytes);
+    auto it = s->idle.lower_bound(need_bytes);
+    if (it != s->idle.end() && it->first <= 2 * need_bytes) {
         *ws = it->second;
         *bytes = it->first;
         s->idle.erase(it);
@@ -370,8 +387,12 @@ void worker_main(zkx_rd_server_s* s)
         bool with_rd = false;
         int staged = 0;
         Layout l{};
+        const long long cells = (long long)head->r.num_pulses * head->r.samples_per_pulse;
         for (Request* q : s->pending) {
             if ((int)group.size() >= s->d.max_batch) break;
+            // CPIs this large keep the GPU (and a host link) busy on their own: fusing more of
+            // them only makes the first ones wait for the last
+            if (!group.empty() && (long long)(group.size() + 1) * cells > kMaxBatchCells) break;
             if (!(q->key == head->key)) continue;
             const int st = staged + (q->x_on_device ? 0 : 1);
             const Layout trial = batch_layout(head->r.num_pulses, head->r.samples_per_pulse,
