@@ -15,11 +15,24 @@
 namespace zkx {
 namespace {
 
-// row[k] = (k < nb ? b[k] / N : 0) + 0i, the scaled, zero-padded taps before their FFT
-__global__ void fir_taps_row_kernel(const float* __restrict__ b, int nb, int N, float2* __restrict__ row)
+// H = FFT(b zero-padded to N) / N in one CTA (real taps, imaginary parts zero).
+template <int N>
+__global__ void __launch_bounds__(FftPlan<N, elems_for(N)>::T)
+fir_spectrum_kernel(const float* __restrict__ b, int nb, float2* __restrict__ H, const float2* __restrict__ tw)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < N) row[k] = make_float2(k < nb ? b[k] / (float)N : 0.f, 0.f);
+    using PL = FftPlan<N, elems_for(N)>;
+    extern __shared__ float2 sm[];
+    const int t = threadIdx.x;
+    constexpr float scale = 1.0f / (float)N;  // exact: N is a power of two
+    float2 v[PL::E];
+#pragma unroll
+    for (int r = 0; r < PL::E; ++r) {
+        const int e = t + PL::T * r;
+        v[r] = make_float2(e < nb ? b[e] * scale : 0.f, 0.f);
+    }
+    fft_block<PL, -1, 1>(v, sm, t, tw);
+#pragma unroll
+    for (int r = 0; r < PL::E; ++r) H[t + PL::T * r] = v[r];
 }
 
 template <int N, int G>
@@ -83,9 +96,11 @@ int fir_fft_impl(const float* b, int nb, const float* x, int lines, int n, const
     ws.stream = s;
     ZKX_TRY(stream_workspace((size_t)N * sizeof(float2), s, &ws.ptr));
     float2* H = static_cast<float2*>(ws.ptr);
-    fir_taps_row_kernel<<<(N + 255) / 256, 256, 0, s>>>(b, nb, N, H);
-    ZKX_LAUNCHED("fir_taps_row_kernel");
-    ZKX_TRY(launch_fft_rows(H, 1, N, 0, H, s));
+    const size_t spec_smem = (size_t)PL::smem_elems() * sizeof(float2);
+    ZKX_CUDA(cudaFuncSetAttribute(fir_spectrum_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)spec_smem));
+    fir_spectrum_kernel<N><<<1, PL::T, spec_smem, s>>>(b, nb, H, twiddle_table());
+    ZKX_LAUNCHED("fir_spectrum_kernel");
     constexpr int G = rows_per_cta(N);
     const size_t smem = (size_t)G * PL::smem_elems() * sizeof(float2);
     auto k = fir_fft_kernel<N, G>;
