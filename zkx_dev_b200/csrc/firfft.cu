@@ -36,7 +36,7 @@ fir_spectrum_kernel(const float* __restrict__ b, int nb, float2* __restrict__ H,
 }
 
 template <int N, int G>
-__global__ void __launch_bounds__(G * FftPlan<N, elems_for(N)>::T)
+__global__ void __launch_bounds__(G * FftPlan<N, elems_for(N)>::T, G * FftPlan<N, elems_for(N)>::T <= 256 ? 3 : 1)
 fir_fft_kernel(const float* __restrict__ x, int lines, int n, int nb, const float2* __restrict__ H,
                const float* __restrict__ zi, float* __restrict__ y, const float2* __restrict__ tw)
 {
