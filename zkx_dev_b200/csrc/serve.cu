@@ -81,8 +81,8 @@ struct Request {
 };
 
 constexpr size_t kAlign = 256;
-// Cells per fused batch (two 1024 x 16384 CPIs): small CPIs batch up to max_batch, large ones
-// run alone.
+// Host-resident cells per fused batch (two 1024 x 16384 CPIs): small CPIs batch up to max_batch,
+// large ones cross the host link alone.
 constexpr long long kMaxBatchCells = 1LL << 25;
 size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 
@@ -390,10 +390,10 @@ void worker_main(zkx_rd_server_s* s)
         const long long cells = (long long)head->r.num_pulses * head->r.samples_per_pulse;
         for (Request* q : s->pending) {
             if ((int)group.size() >= s->d.max_batch) break;
-            // CPIs this large keep the GPU (and a host link) busy on their own: fusing more of
-            // them only makes the first ones wait for the last
-            if (!group.empty() && (long long)(group.size() + 1) * cells > kMaxBatchCells) break;
             if (!(q->key == head->key)) continue;
+            // host-resident CPIs this large keep the host link busy on their own: fusing more
+            // of them only makes the first ones wait for the last copy
+            if (!group.empty() && !q->x_on_device && (long long)(staged + 1) * cells > kMaxBatchCells) break;
             const int st = staged + (q->x_on_device ? 0 : 1);
             const Layout trial = batch_layout(head->r.num_pulses, head->r.samples_per_pulse,
                                               (int)group.size() + 1, st, with_rd || q->r.rd, compat);
