@@ -277,6 +277,14 @@ ZKX_API int zkx_firfilter2_f32(const float* b, int nb, const float* x, int lines
                                int has_padlen, int padlen, int pad_rounding, float* y,
                                zkx_stream_t stream);
 
+/* zkx_firfilter2_f32 with an explicit method (ZKX_FIR_AUTO / DIRECT / FFT).  With padding at
+ * least as long as the filter (padlen >= nb, as the default 3 nb is) the result is one
+ * convolution of the padded line with the taps' autocorrelation, which the FFT method evaluates
+ * by overlap-save; ZKX_FIR_FFT with shorter padding returns ZKX_UNSUPPORTED_OPERATION. */
+ZKX_API int zkx_firfilter2_ex_f32(const float* b, int nb, const float* x, int lines, int n, int padtype,
+                                  int has_padlen, int padlen, int pad_rounding, float* y, int method,
+                                  zkx_stream_t stream);
+
 /* Analytic signal along the last axis of [lines, n]: x zero-padded or truncated to nfft
  * (-1 = n), DFT, one-sided mask, inverse DFT; y is complex64 [lines, nfft].  nfft a power
  * of two up to 65536 or any length up to 32768.  Replaces cusignal::hilbert_device

@@ -170,3 +170,31 @@ def test_hilbert_axis0_and_empty(z):
     assert empty.shape == (3, 8) and not np.any(empty)
     with pytest.raises(ValueError):
         z.hilbert(dev(np.zeros((3, 0), np.float32)))
+
+
+@pytest.mark.parametrize("nb,lines,n,padtype,padlen", [(127, 4, 20000, "odd", None), (16, 3, 5000, "even", None),
+                                                       (255, 1, 9000, "constant", 300), (64, 5, 4000, "odd", 64),
+                                                       (1000, 2, 10000, "odd", None), (2000, 1, 30000, "even", None),
+                                                       (4096, 1, 20000, "odd", 5000), (33, 300, 257, "odd", None),
+                                                       (127, 3, 382, "odd", None)])
+def test_firfilter2_fft_evaluation(z, nb, lines, n, padtype, padlen):
+    """One overlap-save convolution with the taps' autocorrelation (padding >= taps) equals the
+    two-pass definition: against the restatement and the direct kernel."""
+    rng = np.random.default_rng(nb * 3 + n)
+    b = (rng.standard_normal(nb) / np.sqrt(nb)).astype(np.float32)
+    x = rng.standard_normal((lines, n)).astype(np.float32)
+    ref = O.firfilter2(b, x, padtype, padlen)
+    got = z.firfilter2(dev(b), dev(x), padtype=padtype, padlen=padlen, evaluation="fft").cpu().numpy()
+    direct = z.firfilter2(dev(b), dev(x), padtype=padtype, padlen=padlen, evaluation="direct").cpu().numpy()
+    assert rel_l2(got, ref) <= REL_L2
+    assert rel_l2(direct, ref) <= REL_L2
+
+
+def test_firfilter2_fft_needs_padding_as_long_as_the_filter(z):
+    b = dev(np.ones(9, np.float32))
+    x = dev(np.ones((1, 100), np.float32))
+    with pytest.raises(z.ZkxError):
+        z.firfilter2(b, x, padlen=4, evaluation="fft")
+    # the automatic choice falls back to the direct passes
+    got = z.firfilter2(b, x, padlen=4).cpu().numpy()
+    assert rel_l2(got, O.firfilter2(np.ones(9, np.float32), np.ones((1, 100), np.float32), "odd", 4)) <= REL_L2

@@ -96,6 +96,7 @@ SIGNATURES = {
     "zkx_fir_f32": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P]),
     "zkx_fir_ex_f32": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _I, _P]),
     "zkx_firfilter2_f32": (_I, [_P, _I, _P, _I, _I, _I, _I, _I, _I, _P, _P]),
+    "zkx_firfilter2_ex_f32": (_I, [_P, _I, _P, _I, _I, _I, _I, _I, _I, _P, _I, _P]),
     "zkx_hilbert_f32": (_I, [_P, _I, _I, _I, _P, _P]),
     "zkx_upfirdn_length": (ctypes.c_longlong, [_I, _I, _I, _I]),
     "zkx_upfirdn_f32": (_I, [_P, _I, _P, _I, _I, _I, _I, _P, _P]),

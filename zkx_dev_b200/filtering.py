@@ -161,13 +161,17 @@ _PADTYPES = {"odd": L.PAD_ODD, "even": L.PAD_EVEN, "constant": L.PAD_CONSTANT, N
 
 def firfilter2(b: torch.Tensor, x: torch.Tensor, axis: int = -1, padtype: Optional[str] = "odd",
                padlen: Optional[int] = None, method: str = "pad", irlen: Optional[int] = None,
-               pad_rounding: int = 0) -> torch.Tensor:
+               pad_rounding: int = 0, evaluation: str = "auto") -> torch.Tensor:
     """Zero-phase FIR along ``axis`` (cuSignal ``firfilter2(b, x, axis=-1, padtype='odd',
     padlen=None, method='pad', irlen=None)``; filtering_typed.cpp:1226-1302, 1631-1730):
     reflection padding by ``padlen`` samples (default 3 * len(b)), forward and backward FIR
     with steady-state initial conditions, crop.  ``irlen`` is ignored by the pad method, as
     in the reference; ``method='gust'`` is not supported there either.  ``pad_rounding``
-    (``L.PAD_ROUND_*``) rounds odd-reflected pad values as a half / integer input would."""
+    (``L.PAD_ROUND_*``) rounds odd-reflected pad values as a half / integer input would.
+    ``evaluation``: "direct" (forward and backward passes), "fft" (one overlap-save
+    convolution with the taps' autocorrelation; needs padlen >= len(b)) or "auto"."""
+    if evaluation not in _FIR_METHODS:
+        raise ValueError("firfilter2 evaluation")
     if method == "gust":
         raise ValueError("firfilter2 gust is not supported by cuSignal 23.08.00")
     if method != "pad":
@@ -182,9 +186,9 @@ def firfilter2(b: torch.Tensor, x: torch.Tensor, axis: int = -1, padtype: Option
     n = xm.shape[-1]
     lines = xm.numel() // n if n else 0
     y = torch.empty_like(xm)
-    L.check(L.lib().zkx_firfilter2_f32(b.data_ptr(), b.numel(), xm.data_ptr(), lines, n, _PADTYPES[padtype],
-                                       int(padlen is not None), int(padlen or 0), int(pad_rounding),
-                                       y.data_ptr(), L.stream_handle()))
+    L.check(L.lib().zkx_firfilter2_ex_f32(b.data_ptr(), b.numel(), xm.data_ptr(), lines, n, _PADTYPES[padtype],
+                                          int(padlen is not None), int(padlen or 0), int(pad_rounding),
+                                          y.data_ptr(), _FIR_METHODS[evaluation], L.stream_handle()))
     return _from_last(y, ax, x.ndim)
 
 
