@@ -519,6 +519,63 @@ def run_serving(dev, n_requests: int = 256, pool: int = 24, seconds: float = 2.0
     return res
 
 
+def run_serving_sweep(dev, rates=(500, 1000, 1500, 2000), seconds: float = 1.5, pool: int = 24) -> dict:
+    """Poisson arrivals of device-resident CPIs at several rates: the mixed-size stream
+    (pulses 2^U{6..10}, range 2^U{10..15}, chirp range/16) with 10 % large 2048 x 65536 CPIs,
+    all generated on the device.  Per rate: completed CPIs/s and latency p50/p99/max (submit ->
+    mask in the caller's device buffer)."""
+    import random
+    import torch
+    import zkx_dev_b200 as z
+    from zkx_dev_b200 import synth
+
+    rng = np.random.default_rng(synth.seed_for(5, 0))
+    shapes = [(int(2 ** rng.integers(6, 11)), int(2 ** rng.integers(10, 16))) for _ in range(pool)]
+    shapes += [(2048, 65536)] * 2
+    cpis, replicas = [], {}
+    for i, (P_, N_) in enumerate(shapes):
+        L_ = N_ // 16
+        targets = synth.draw_targets(P_, N_, int(rng.integers(5, 51)), L_, synth.seed_for(5, i + 1))
+        cpis.append(synth.device_cpi(P_, N_, targets, L_, synth.seed_for(5, i + 101)))
+        if (P_, N_) not in replicas:
+            replicas[(P_, N_)] = torch.as_tensor(synth.lfm_chirp(L_).astype(np.complex64), device=dev)
+    dets = [torch.empty(c.shape, dtype=torch.uint8, device=dev) for c in cpis]
+    small, large = list(range(pool)), [pool, pool + 1]
+    prng = random.Random(13)
+
+    def pick():
+        return prng.choice(large) if prng.random() < 0.1 else prng.choice(small)
+
+    res = {"workload": ("Poisson arrivals, device-resident CPIs: pulses 2^U{6..10} x range 2^U{10..15} "
+                        "plus 10% 2048x65536, chirp range/16, 5-50 targets"), "seconds_per_rate": seconds,
+           "rates": []}
+    with z.RdServer(z.ServerConfig()) as server:
+        def submit(k):
+            P_, N_ = cpis[k].shape
+            return server.submit(cpis[k], replicas[(P_, N_)], P_ * 100000 + N_, dets[k])
+        for _ in range(2):   # plans and the workspaces of the batch sizes bursts form
+            for t in [submit(pick()) for _ in range(4 * len(cpis))]:
+                server.wait(t)
+        for rate in rates:
+            server.reset_stats()
+            tickets = []
+            t_next = time.perf_counter()
+            t_end = t_next + seconds
+            while t_next < t_end:
+                while time.perf_counter() < t_next:
+                    pass
+                tickets.append(submit(pick()))
+                t_next += prng.expovariate(rate)
+            for t in tickets:
+                server.wait(t)
+            st = server.stats()
+            res["rates"].append({"offered_cpis_per_s": rate, "completed": int(st["completed"]),
+                                 "cpis_per_s": round(st["cpis_per_s"], 1),
+                                 "p50_ms": round(st["p50_us"] / 1e3, 3), "p99_ms": round(st["p99_us"] / 1e3, 3),
+                                 "max_ms": round(st["max_us"] / 1e3, 3)})
+    return res
+
+
 def chain_spectrum(chain) -> int:
     """Device pointer of a plan's resident replica spectrum, via a fresh spectrum call
     with the plan's settings (kept alive on the chain object)."""
@@ -652,6 +709,7 @@ def main() -> None:
         if world == 1 and not args.no_serving:
             import torch
             line["serving"] = run_serving(torch.device("cuda", 0))
+            line["serving"]["sweep"] = run_serving_sweep(torch.device("cuda", 0))
         if world == 1 and not args.no_cpu_baseline:
             base = reference_cpu_baseline(1, 0)
             line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}

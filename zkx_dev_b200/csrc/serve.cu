@@ -84,6 +84,8 @@ constexpr size_t kAlign = 256;
 // Host-resident cells per fused batch (two 1024 x 16384 CPIs): small CPIs batch up to max_batch,
 // large ones cross the host link alone.
 constexpr long long kMaxBatchCells = 1LL << 25;
+// Cells per fused batch of any CPIs (one 2048 x 65536 CPI).
+constexpr long long kMaxFusedCells = 1LL << 27;
 size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 
 // Workspace of one batch of `count` CPIs [P, N] (range nfft N, Doppler nfft P), of which
@@ -391,6 +393,9 @@ void worker_main(zkx_rd_server_s* s)
         for (Request* q : s->pending) {
             if ((int)group.size() >= s->d.max_batch) break;
             if (!(q->key == head->key)) continue;
+            // a batch stays within the kernels' int indexing, and CPIs this large fill the GPU
+            // on their own (their workspaces would only grow)
+            if (!group.empty() && (long long)(group.size() + 1) * cells > kMaxFusedCells) break;
             // host-resident CPIs this large keep the host link busy on their own: fusing more
             // of them only makes the first ones wait for the last copy
             if (!group.empty() && !q->x_on_device && (long long)(staged + 1) * cells > kMaxBatchCells) break;
