@@ -420,6 +420,7 @@ def run_serving(dev, n_requests: int = 256, pool: int = 24, seconds: float = 2.0
     length range/16, Hamming windows, CFAR guard 2x2 train 8x8 Pfa 1e-6.  A pool of `pool`
     seeded CPIs is drawn from that distribution and `n_requests` requests are drawn from
     the pool.  Measures (1) the plain path, one CPI per launch sequence on one stream,
+    (1b) the same requests grouped by shape into stacked batches captured as one CUDA graph,
     (2) the serving loop on device-resident buffers and (3) with page-locked host
     buffers (copies included), all submitted at once, then (4) the serving loop under
     Poisson arrivals at 70 % of (3)'s rate for `seconds`, for its latency."""
@@ -460,6 +461,35 @@ def run_serving(dev, n_requests: int = 256, pool: int = 24, seconds: float = 2.0
     b.record()
     b.synchronize()
     plain = n_requests / (a.elapsed_time(b) * 1e-3)
+
+    # (1b) the uneven batch as one CUDA graph: the requests grouped by shape, each group one
+    # stacked batch (one launch per stage), every group captured into a single graph
+    groups = {}
+    for k in order:
+        groups.setdefault(cpis[k].x.shape, []).append(k)
+    stacked = []
+    for shp, ks in groups.items():
+        ch, _ = chains[shp]
+        xb = torch.stack([dev_x[k] for k in ks])
+        ob = ch.allocate_outputs(keep_compressed=False, keep_rd=False, batch=len(ks))
+        ch.run_batch(xb, ob)                         # plan-owned buffers sized before capture
+        stacked.append((ch, xb, ob))
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        for ch, xb, ob in stacked:
+            ch.run_batch(xb, ob)
+    for _ in range(3):
+        graph.replay()
+    torch.cuda.synchronize()
+    a.record()
+    reps = 5
+    for _ in range(reps):
+        graph.replay()
+    b.record()
+    b.synchronize()
+    uneven_graph = reps * n_requests / (a.elapsed_time(b) * 1e-3)
+    del graph, stacked
     for ch, _ in chains.values():
         ch.close()
 
@@ -504,6 +534,8 @@ def run_serving(dev, n_requests: int = 256, pool: int = 24, seconds: float = 2.0
                      "2^U{6..10}, range 2^U{10..15}, chirp range/16, 5-50 targets"),
         "cells": cells,
         "plain_device_cpis_per_s": round(plain, 1),
+        "uneven_graph_cpis_per_s": round(uneven_graph, 1),
+        "uneven_graph_shapes": len(groups),
         "served_device_cpis_per_s": round(st_dev["cpis_per_s"], 1),
         "served_vs_plain_device": round(st_dev["cpis_per_s"] / plain, 3),
         "served_device_gbs": round(st_dev["cpis_per_s"] * cells / n_requests * 45 / 1e9, 1),
