@@ -551,6 +551,59 @@ def run_serving(dev, n_requests: int = 256, pool: int = 24, seconds: float = 2.0
     return res
 
 
+def run_precision(dev) -> dict:
+    """The precision comparison: one 512 x 8192 CPI (40 targets, chirp 512, 5 % of the targets
+    at 0-3 dB SNR near the threshold), the chain with range compression in plain FP32 and as
+    tensor-core DFT GEMMs with split hi+lo FP16 / BF16 operands, against a full FP64 chain
+    (numpy): relative L2 and max |error| / max |reference| of the compressed cube and of the
+    power map, and detection-mask cells that differ from the FP64 chain's CA-CFAR."""
+    import torch
+    import zkx_dev_b200 as z
+    from zkx_dev_b200 import synth
+    P_, N_, L_ = 512, 8192, 512
+    cpi = synth.make_cpi(P_, N_, 40, L_, synth.seed_for(3, 0), low_snr_fraction=0.05, low_snr_db=(0.0, 3.0))
+    h = cpi.replica.astype(np.complex128) * hamming_f32(L_)
+    h /= np.linalg.norm(h)
+    comp64 = np.fft.ifft(np.fft.fft(cpi.x.astype(np.complex128), axis=1) * np.conj(np.fft.fft(h, N_)), axis=1)
+    pow64 = np.abs(np.fft.fft(comp64 * hamming_f32(P_)[:, None], axis=0)) ** 2
+    gr, gc, tr, tc = 2, 2, 8, 8
+    nref = (2 * (gr + tr) + 1) * (2 * (gc + tc) + 1) - (2 * gr + 1) * (2 * gc + 1)
+    alpha = nref * (1e-6 ** (-1.0 / nref) - 1.0)
+    cum = np.zeros((P_ + 1, N_ + 1))
+    cum[1:, 1:] = np.cumsum(np.cumsum(pow64, axis=0), axis=1)
+
+    def box(r0, r1, c0, c1):  # sums of pow64[r0:r1, c0:c1] for arrays of corners
+        return cum[r1, c1] - cum[r0, c1] - cum[r1, c0] + cum[r0, c0]
+
+    rr, cc = np.meshgrid(np.arange(gr + tr, P_ - gr - tr), np.arange(gc + tc, N_ - gc - tc), indexing="ij")
+    outer = box(rr - gr - tr, rr + gr + tr + 1, cc - gc - tc, cc + gc + tc + 1)
+    inner = box(rr - gr, rr + gr + 1, cc - gc, cc + gc + 1)
+    mask64 = pow64[rr, cc] > alpha / nref * (outer - inner)
+
+    def rel(a, b):
+        return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+    res = {"workload": "512x8192 CPI, 40 targets (5% at 0-3 dB), chirp 512, Hamming, CFAR 2x2/8x8 1e-6",
+           "reference": "FP64 chain (numpy)"}
+    x = torch.as_tensor(cpi.x, device=dev)
+    for prec in ("fp32", "tc_f16", "tc_bf16"):
+        chain = z.RangeDopplerChain(z.ChainConfig(P_, N_, L_, pfa=1e-6, precision=prec),
+                                    torch.as_tensor(cpi.replica, device=dev))
+        out = chain.run(x)
+        torch.cuda.synchronize()
+        comp = out["compressed"].cpu().numpy().astype(np.complex128)
+        power = out["power"].cpu().numpy().astype(np.float64)
+        det = out["detections"].cpu().numpy()[rr, cc].astype(bool)
+        res[prec] = {"compressed_rel_l2": rel(comp, comp64),
+                     "compressed_max_rel": float(np.max(np.abs(comp - comp64)) / np.max(np.abs(comp64))),
+                     "power_rel_l2": rel(power, pow64),
+                     "power_max_rel": float(np.max(np.abs(power - pow64)) / np.max(pow64)),
+                     "mask_cells_differing_from_fp64": int(np.sum(det != mask64)),
+                     "detections": int(det.sum()), "detections_fp64": int(mask64.sum())}
+        chain.close()
+    return res
+
+
 def run_serving_sweep(dev, rates=(500, 1000, 1500, 2000), seconds: float = 1.5, pool: int = 24) -> dict:
     """Poisson arrivals of device-resident CPIs at several rates: the mixed-size stream
     (pulses 2^U{6..10}, range 2^U{10..15}, chirp range/16) with 10 % large 2048 x 65536 CPIs,
@@ -742,6 +795,7 @@ def main() -> None:
             import torch
             line["serving"] = run_serving(torch.device("cuda", 0))
             line["serving"]["sweep"] = run_serving_sweep(torch.device("cuda", 0))
+            line["precision"] = run_precision(torch.device("cuda", 0))
         if world == 1 and not args.no_cpu_baseline:
             base = reference_cpu_baseline(1, 0)
             line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
