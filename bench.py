@@ -741,6 +741,9 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the mixed-stream serving measurement")
+    ap.add_argument("--serving-only", action="store_true",
+                    help="print only the serving measurements as JSON (run in a fresh process by "
+                         "the default invocation)")
     ap.add_argument("--profile", action="store_true",
                     help="one input set, one warm-up and one step of every stage, no timing "
                          "(the command profiled under ncu)")
@@ -749,6 +752,14 @@ def main() -> None:
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.serving_only:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        serving = run_serving(dev)
+        serving["sweep"] = run_serving_sweep(dev)
+        print(json.dumps(serving))
+        return
     config = {"workload": WORKLOAD, "pulses": P, "range": NR, "chirp": L, "targets": N_TARGETS,
               "front_end": f"{CH}x{NS} fir{FIR_TAPS} resample {UP}/{DOWN}",
               "cfar": "guard 2x2 train 8x8 pfa 1e-6", "parallelism": f"replicas{world}",
@@ -793,8 +804,14 @@ def main() -> None:
                 "rel_err_vs_fp64": res["rel_err_vs_fp64"], "tuning": res["tuning"]}
         if world == 1 and not args.no_serving:
             import torch
-            line["serving"] = run_serving(torch.device("cuda", 0))
-            line["serving"]["sweep"] = run_serving_sweep(torch.device("cuda", 0))
+            # the serving loop in a process of its own: its host threads and allocations start
+            # from a clean process rather than after the step benchmark's
+            r = subprocess.run([sys.executable, os.path.abspath(__file__), "--serving-only"],
+                               capture_output=True, text=True, timeout=900)
+            try:
+                line["serving"] = json.loads(r.stdout.strip().splitlines()[-1])
+            except (IndexError, ValueError):
+                line["serving"] = {"error": (r.stderr or "no output").strip().splitlines()[-1][:300]}
             line["precision"] = run_precision(torch.device("cuda", 0))
         if world == 1 and not args.no_cpu_baseline:
             base = reference_cpu_baseline(1, 0)

@@ -278,9 +278,11 @@ int issue_batch(zkx_rd_server_s* s, const PlanEntry& pe, Batch* b, const Layout&
 
 // A workspace block of at least `need_bytes` for a batch admitted under the budget; called
 // by the worker with the lock held, which it drops around allocation and release calls.
-// An idle block of up to twice the size is reused; otherwise idle blocks are released
-// (largest first) until a new block of the size class fits within the budget next to the
-// blocks in use.
+// The smallest idle block that is large enough is reused, so that after the first batches the
+// server holds about max_inflight blocks of the largest sizes and allocates nothing more (an
+// allocation of gigabytes in the middle of a stream stalls every request behind it);
+// otherwise idle blocks are released (largest first) until a new block of the size class fits
+// within the budget next to the blocks in use.
 // Block sizes are rounded up to classes 2^k * {1, 1.25, 1.5, 1.75} (at least 1 MB), so that the
 // varying batch compositions of a request stream keep reusing a few blocks instead of
 // allocating new ones (an allocation can stall the device).
@@ -298,7 +300,7 @@ int acquire_block(zkx_rd_server_s* s, std::unique_lock<std::mutex>& lk, size_t n
 {
     const size_t need = size_class(need_bytes);
     auto it = s->idle.lower_bound(need_bytes);
-    if (it != s->idle.end() && it->first <= 2 * need_bytes) {
+    if (it != s->idle.end()) {
         *ws = it->second;
         *bytes = it->first;
         s->idle.erase(it);
