@@ -198,3 +198,28 @@ def test_firfilter2_fft_needs_padding_as_long_as_the_filter(z):
     # the automatic choice falls back to the direct passes
     got = z.firfilter2(b, x, padlen=4).cpu().numpy()
     assert rel_l2(got, O.firfilter2(np.ones(9, np.float32), np.ones((1, 100), np.float32), "odd", 4)) <= REL_L2
+
+
+def test_hilbert_of_a_cosine_is_the_complex_exponential(z):
+    """For a cosine on an exact bin, the analytic signal is exp(i w n): real part the cosine,
+    imaginary part the sine (cuSignal's hilbert contract)."""
+    n = np.arange(4096)
+    for k in (1, 17, 1000, 2047):
+        x = np.cos(2 * np.pi * k * n / 4096).astype(np.float32)
+        got = z.hilbert(dev(x[None, :])).cpu().numpy()[0]
+        ref = np.exp(1j * 2 * np.pi * k * n / 4096)
+        assert rel_l2(got, ref) <= REL_L2, k
+
+
+def test_firfilter2_has_zero_phase(z):
+    """A passband sinusoid comes out of the zero-phase filter with no delay: the output equals
+    the input times |H(w)|^2 away from the line ends."""
+    from zkx_dev_b200.synth import firwin_kaiser
+    b = firwin_kaiser(63, 0.3, 8.0).astype(np.float32)
+    n = np.arange(20000)
+    w = 2 * np.pi * 0.05
+    x = np.cos(w * n + 0.3).astype(np.float32)
+    got = z.firfilter2(dev(b), dev(x[None, :])).cpu().numpy()[0]
+    gain = np.abs(np.sum(b.astype(np.float64) * np.exp(-1j * w * np.arange(63)))) ** 2
+    mid = slice(2000, 18000)
+    assert rel_l2(got[mid], gain * x[mid].astype(np.float64)) <= 1e-4
