@@ -261,6 +261,36 @@ __device__ __forceinline__ void apply_twiddles(float2* v, int n, const float2* _
     }
 }
 
+// The same product with W_Mprev^(n k) read from a per-CTA shared table tab[n (R + 1) + k]
+// (n < M of the pass; the odd row pitch keeps the lanes' reads on distinct banks).
+template <int R, int DIR>
+__device__ __forceinline__ void apply_twiddles_table(float2* v, int n, const float2* tab)
+{
+    const float2* row = tab + n * (R + 1);
+    static_for<1, R>([&](auto K) {
+        constexpr int k = decltype(K)::value;
+        float2 w = row[k];
+        if constexpr (DIR > 0) w = cconj(w);
+        v[k] = cmul(v[k], w);
+    });
+}
+
+// Rows n < PL::M(2) of the table apply_twiddles_table reads in the second pass of a
+// three-pass plan: tab[n (E + 1) + k] = W_M(1)^(n k).  Callers size it mid_table_elems().
+template <class PL>
+constexpr int mid_table_elems() { return PL::PASSES == 3 ? PL::M(2) * (PL::E + 1) : 0; }
+
+template <class PL>
+__device__ __forceinline__ void fill_mid_table(float2* tab, int t, int nthreads, const float2* __restrict__ tw)
+{
+    constexpr int P = PL::E + 1;
+    for (int i = t; i < mid_table_elems<PL>(); i += nthreads) {
+        const int n = i / P, k = i - n * P;
+        const unsigned idx = ((unsigned)(n * k) << (kTwiddleLog - PL::LOGM(1))) & (kTwiddleSize - 1);
+        tab[i] = k < PL::E ? tw[idx] : make_float2(0.f, 0.f);
+    }
+}
+
 // One transform of length PL::N.  On entry v[r] holds element t + T*r, on exit
 // v[r] holds output bin t + T*r.  sm points at this transform's exchange buffer;
 // element a of the buffer lives at sm[a * C].  The caller must __syncthreads()
@@ -268,7 +298,7 @@ __device__ __forceinline__ void apply_twiddles(float2* v, int n, const float2* _
 // must call this (it synchronises the block).
 template <class PL, int DIR, int C, bool PAD = true>
 __device__ __forceinline__ void fft_block(float2 (&v)[PL::E], float2* sm, int t,
-                                          const float2* __restrict__ tw)
+                                          const float2* __restrict__ tw, const float2* mid = nullptr)
 {
     constexpr int E = PL::E;
     constexpr int T = PL::T;
@@ -298,7 +328,10 @@ __device__ __forceinline__ void fft_block(float2 (&v)[PL::E], float2* sm, int t,
             });
             __syncthreads();
             dft<E, DIR>(v);
-            apply_twiddles<E, DIR, PL::LOGM(i - 1)>(v, n, tw);
+            if (i == 2 && mid != nullptr)
+                apply_twiddles_table<E, DIR>(v, n, mid);
+            else
+                apply_twiddles<E, DIR, PL::LOGM(i - 1)>(v, n, tw);
             static_for<0, E>([&](auto K) {
                 constexpr int k = decltype(K)::value;
                 sm[padded<PL, i, PAD>((s + Pprev * k) * Mi + n) * C] = v[k];

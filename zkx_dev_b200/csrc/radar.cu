@@ -123,7 +123,10 @@ pulse_compression_persistent_kernel(const Src src, int pulses, int samples,
     using PL = FftPlan<N, elems_for(N)>;
     extern __shared__ __align__(128) float2 sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + PL::smem_elems());
+    // second-pass twiddles, the same for every pulse the CTA transforms
+    float2* mid = mid_table_elems<PL>() > 0 ? sm + PL::smem_elems() + 2 : nullptr;
     const int t = threadIdx.x;
+    if (mid) fill_mid_table<PL>(mid, t, PL::T, tw);
     const int copy = samples < N ? samples : N;                 // elements staged per pulse
     const uint32_t bytes = (uint32_t)copy * (uint32_t)sizeof(float2);
     constexpr uint32_t kChunk = 32768;                          // bytes per bulk copy
@@ -160,11 +163,11 @@ pulse_compression_persistent_kernel(const Src src, int pulses, int samples,
             v[r] = e < copy ? sm[e] : make_float2(0.f, 0.f);
         }
         __syncthreads();
-        fft_block<PL, -1, 1>(v, sm, t, tw);
+        fft_block<PL, -1, 1>(v, sm, t, tw, mid);
 #pragma unroll
         for (int r = 0; r < PL::E; ++r) v[r] = cmul(v[r], __ldg(&spectrum[t + PL::T * r]));
         __syncthreads();
-        fft_block<PL, 1, 1>(v, sm, t, tw);
+        fft_block<PL, 1, 1>(v, sm, t, tw, mid);
         // every thread is done with the exchange buffer; order those accesses before the
         // bulk copy that overwrites it
         fence_proxy_async_smem();
@@ -375,7 +378,7 @@ int compression_impl(const Src& x, bool aligned16, int pulses, int samples, cons
             int dev = 0, sms = 0;
             ZKX_CUDA(cudaGetDevice(&dev));
             ZKX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            const size_t smem = (size_t)PL::smem_elems() * sizeof(float2) + 16;
+            const size_t smem = ((size_t)PL::smem_elems() + 2 + mid_table_elems<PL>()) * sizeof(float2);
             auto k = pulse_compression_persistent_kernel<N, Src>;
             ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             int per_sm = 0;
