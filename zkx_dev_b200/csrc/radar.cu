@@ -73,6 +73,14 @@ replica_spectrum_kernel(const float2* __restrict__ h, int length, int normalize,
 
 // ------------------------------------------------------------ range compression
 
+// Range compression lengths with a persistent kernel (N >= 4096) and a three-pass plan
+// read the second-pass twiddles from a shared table in both compression kernels.
+template <int N>
+constexpr bool compression_mid_table()
+{
+    return N >= 4096 && mid_table_elems<FftPlan<N, elems_for(N)>>() > 0;
+}
+
 // G pulses per CTA; each pulse: load (zero-pad/truncate to N), forward FFT, multiply
 // by the replica spectrum, inverse FFT, store.  The cube crosses HBM once each way.
 template <int N, int G, class Src>
@@ -88,6 +96,10 @@ pulse_compression_kernel(const Src src, int pulses, int samples,
     const int pulse = blockIdx.x * G + g;
     const bool active = pulse < pulses;
     float2* smg = sm + g * PL::smem_elems();
+    // lengths that also have the persistent kernel take its second-pass twiddle table,
+    // so both kernels round identically and the tuning choice never changes a result
+    float2* mid = compression_mid_table<N>() ? sm + G * PL::smem_elems() : nullptr;
+    if (mid) fill_mid_table<PL>(mid, threadIdx.x, G * PL::T, tw);
     const float2* xr = active ? src.row(pulse) : nullptr;
     float2 v[PL::E];
 #pragma unroll
@@ -95,11 +107,11 @@ pulse_compression_kernel(const Src src, int pulses, int samples,
         const int e = t + PL::T * r;
         v[r] = (active && e < samples) ? __ldcs(&xr[e]) : make_float2(0.f, 0.f);
     }
-    fft_block<PL, -1, 1>(v, smg, t, tw);
+    fft_block<PL, -1, 1>(v, smg, t, tw, mid);
 #pragma unroll
     for (int r = 0; r < PL::E; ++r) v[r] = cmul(v[r], __ldg(&spectrum[t + PL::T * r]));
     if constexpr (PL::PASSES > 1) __syncthreads();
-    fft_block<PL, 1, 1>(v, smg, t, tw);
+    fft_block<PL, 1, 1>(v, smg, t, tw, mid);
     if (active) {
         float2* yr = y + (size_t)pulse * N;
 #pragma unroll
@@ -391,7 +403,8 @@ int compression_impl(const Src& x, bool aligned16, int pulses, int samples, cons
         }
     }
     constexpr int G = rows_per_cta(N);
-    const size_t smem = (size_t)G * PL::smem_elems() * sizeof(float2);
+    const size_t smem = ((size_t)G * PL::smem_elems() +
+                         (compression_mid_table<N>() ? mid_table_elems<PL>() : 0)) * sizeof(float2);
     auto k = pulse_compression_kernel<N, G, Src>;
     ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int blocks = (pulses + G - 1) / G;
