@@ -14,6 +14,7 @@
 // 2656-2684) without visiting the taps of other phases.  Taps are regrouped per
 // phase in shared memory; the input span of the CTA's outputs is staged once.
 #include "fft_core.cuh"
+#include "tma.cuh"
 #include "zkx_internal.h"
 
 namespace zkx {
@@ -211,60 +212,101 @@ polyphase_kernel(const float* __restrict__ h, int nh, int up, int down, long lon
 
 // Register-blocked polyphase for fixed (UP, DOWN, J): thread (g, r) computes the Q
 // outputs m = m0 + g*UP*Q + r + UP*i, which share one phase, so its J taps and the
-// J + DOWN*(Q-1) input samples they touch stay in registers (each sample is reused by
-// up to J/DOWN outputs).  Outputs are staged in shared memory and stored coalesced.
+// J + DOWN*(Q-1) input samples they touch are read from shared memory once each (each
+// sample is reused by up to J/DOWN outputs).  G groups of UP threads with G*UP*Q a
+// multiple of 4, so a CTA's outputs start on a 16-byte boundary of an aligned row.
+// The input span arrives as one bulk copy (from the 4-sample boundary at or below its
+// first sample) wherever it lies inside the line and the line is 16-byte aligned;
+// spans that reach past either end are gathered with zero fill.  Outputs are staged
+// in shared memory and stored as 128-bit words.
+template <int UP, int Q>
+constexpr int poly_groups()
+{
+    int g = kPolyThreads / UP;
+    while ((g * UP * Q) % 4 != 0) --g;
+    return g;
+}
+
 template <int UP, int DOWN, int J, int Q>
-__global__ void __launch_bounds__((kPolyThreads / UP) * UP)
+struct PolyBlockGeom {
+    static constexpr int NT = poly_groups<UP, Q>() * UP;
+    static constexpr int BLOCK = NT * Q;                         // outputs per CTA
+    static constexpr int HW = (UP * J + 3) & ~3;                 // phase-major taps
+    // samples from floor(qlo) needed by the CTA: newest index (rb + (BLOCK-1)*DOWN)/UP
+    // + J - 1 relative to qlo, plus up to 3 of alignment, rounded to 4
+    static constexpr int SPAN = ((BLOCK * DOWN) / UP + J + 2 + 3 + 3) & ~3;
+    static constexpr size_t smem_bytes() { return (size_t)(4 + HW + BLOCK + SPAN) * sizeof(float); }
+};
+
+template <int UP, int DOWN, int J, int Q>
+__global__ void __launch_bounds__(PolyBlockGeom<UP, DOWN, J, Q>::NT)
 polyphase_blocked_kernel(const float* __restrict__ h, int nh, long long offset,
                          const float* __restrict__ x, int n, float* __restrict__ y, int nout,
-                         int span_cap)
+                         int aligned, int* err)
 {
-    constexpr int G = kPolyThreads / UP;
-    constexpr int NT = G * UP;
-    constexpr int BLOCK = NT * Q;
-    constexpr int W = J + DOWN * (Q - 1);
-    extern __shared__ float sm[];
-    float* hp = sm;                              // [UP][J]
-    float* ys = hp + ((UP * J + 3) & ~3);        // BLOCK staged outputs
-    float* xs = ys + BLOCK;                      // input span
+    using PG = PolyBlockGeom<UP, DOWN, J, Q>;
+    constexpr int NT = PG::NT, BLOCK = PG::BLOCK, SPAN = PG::SPAN;
+    extern __shared__ __align__(16) float sm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
+    float* hp = sm + 4;                          // [UP][J]
+    float* ys = hp + PG::HW;                     // BLOCK staged outputs
+    float* xs = ys + BLOCK;                      // xs[k] = sample qa + k
     const int line = blockIdx.y;
     const long long m0 = (long long)blockIdx.x * BLOCK;
     const long long base = m0 * DOWN + offset;
     const long long qb = floor_div(base, UP);
     const int rb = (int)(base - qb * UP);
     const long long qlo = qb - (J - 1);
+    const long long qa = qlo & ~3LL;             // 4-sample boundary at or below qlo
+    const int shift = (int)(qlo - qa);
     const float* xl = x + (size_t)line * n;
+    const bool bulk = (aligned & 1) && qa >= 0 && qa + SPAN <= n;
+    if (bulk && threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_arrive_expect_tx(bar, (uint32_t)(SPAN * sizeof(float)));
+        bulk_load_1d(xs, xl + qa, (uint32_t)(SPAN * sizeof(float)), bar);
+    }
     for (int i = threadIdx.x; i < UP * J; i += NT) {
         const int ph = i / J, j = i - ph * J;
         const int k = ph + j * UP;
         hp[i] = k < nh ? h[k] : 0.f;
     }
-    for (int i0 = 0; i0 < span_cap; i0 += 8 * NT) {
-        float tmp[8];
+    if (!bulk) {
+        for (int i0 = 0; i0 < SPAN; i0 += 8 * NT) {
+            float tmp[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int i = i0 + u * NT + threadIdx.x;
-            const long long s = qlo + i;
-            tmp[u] = (i < span_cap && s >= 0 && s < n) ? __ldcs(&xl[s]) : 0.f;
-        }
+            for (int u = 0; u < 8; ++u) {
+                const int i = i0 + u * NT + threadIdx.x;
+                const long long s = qa + i;
+                tmp[u] = (i < SPAN && s >= 0 && s < n) ? __ldcs(&xl[s]) : 0.f;
+            }
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int i = i0 + u * NT + threadIdx.x;
-            if (i < span_cap) xs[i] = tmp[u];
+            for (int u = 0; u < 8; ++u) {
+                const int i = i0 + u * NT + threadIdx.x;
+                if (i < SPAN) xs[i] = tmp[u];
+            }
         }
     }
     __syncthreads();
+    if (bulk) {
+        const bool ok = mbar_wait_bounded(bar, 0);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
+            return;
+        }
+    }
     const int g = threadIdx.x / UP, r = threadIdx.x - (threadIdx.x / UP) * UP;
     const int d0 = g * UP * Q + r;
     const int t0 = rb + d0 * DOWN;
-    const int q0 = t0 / UP;                      // relative to qb
+    const int q0 = t0 / UP;                      // newest sample of output 0, relative to qb
     const int ph = t0 - q0 * UP;
     float hreg[J];
 #pragma unroll
     for (int j = 0; j < J; ++j) hreg[j] = hp[ph * J + j];
+    constexpr int W = J + DOWN * (Q - 1);
     float xw[W];                                 // xw[w] = sample qb + q0 - (J-1) + w
 #pragma unroll
-    for (int w = 0; w < W; ++w) xw[w] = xs[q0 + w];
+    for (int w = 0; w < W; ++w) xw[w] = xs[shift + q0 + w];
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         float acc = 0.f;
@@ -274,9 +316,15 @@ polyphase_blocked_kernel(const float* __restrict__ h, int nh, long long offset,
     }
     __syncthreads();
     float* yl = y + (size_t)line * nout;
-    for (int i = threadIdx.x; i < BLOCK; i += NT) {
-        const long long m = m0 + i;
-        if (m < nout) __stcs(&yl[m], ys[i]);
+    if ((aligned & 2) && m0 + BLOCK <= nout) {
+        float4* yp = reinterpret_cast<float4*>(yl + m0);
+        const float4* ysp = reinterpret_cast<const float4*>(ys);
+        for (int i = threadIdx.x; i < BLOCK / 4; i += NT) __stcs(&yp[i], ysp[i]);
+    } else {
+        for (int i = threadIdx.x; i < BLOCK; i += NT) {
+            const long long m = m0 + i;
+            if (m < nout) __stcs(&yl[m], ys[i]);
+        }
     }
 }
 
@@ -284,15 +332,14 @@ template <int UP, int DOWN, int J, int Q>
 int polyphase_blocked_launch(const float* taps, int ntaps, long long offset, const float* x,
                              int lines, int n, float* y, int nout, cudaStream_t stream)
 {
-    constexpr int NT = (kPolyThreads / UP) * UP;
-    constexpr int BLOCK = NT * Q;
-    // span: floor((BLOCK-1)*DOWN/UP) + 1 + J samples (+1 slack for the base remainder)
-    const int span_cap = (BLOCK * DOWN) / UP + J + 2;
-    const size_t smem = ((size_t)((UP * J + 3) & ~3) + BLOCK + span_cap) * sizeof(float);
+    using PG = PolyBlockGeom<UP, DOWN, J, Q>;
+    const size_t smem = PG::smem_bytes();
+    const int aligned = (((n & 3) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) ? 1 : 0) |
+                        (((nout & 3) == 0 && (reinterpret_cast<uintptr_t>(y) & 15) == 0) ? 2 : 0);
     auto k = polyphase_blocked_kernel<UP, DOWN, J, Q>;
     ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((unsigned)((nout + BLOCK - 1) / BLOCK), (unsigned)lines);
-    k<<<grid, NT, smem, stream>>>(taps, ntaps, offset, x, n, y, nout, span_cap);
+    dim3 grid((unsigned)((nout + PG::BLOCK - 1) / PG::BLOCK), (unsigned)lines);
+    k<<<grid, PG::NT, smem, stream>>>(taps, ntaps, offset, x, n, y, nout, aligned, kernel_error_word());
     ZKX_LAUNCHED("polyphase_blocked_kernel");
     return ZKX_SUCCESS;
 }
