@@ -56,11 +56,24 @@ fir_fft_kernel(const float* __restrict__ x, int lines, int n, int nb, const floa
     const float* xa = x + (size_t)la * n;
     const float* xb = x + (size_t)(has_b ? lb : la) * n;
     float2 v[PL::E];
+    // blocks wholly inside the line (all but the first and last of each line) load at
+    // constant offsets from the block's first sample, without per-sample range checks
+    if (active && s0 >= 0 && s0 + N <= n) {
+        const float* pa = xa + s0 + t;
+        const float* pb = xb + s0 + t;
 #pragma unroll
-    for (int r = 0; r < PL::E; ++r) {
-        const long long s = s0 + t + PL::T * r;
-        const bool in = active && s >= 0 && s < n;
-        v[r] = make_float2(in ? __ldcs(&xa[s]) : 0.f, (in && has_b) ? __ldcs(&xb[s]) : 0.f);
+        for (int r = 0; r < PL::E; ++r) {
+            const float a = __ldcs(pa + PL::T * r);
+            const float b = __ldcs(pb + PL::T * r);
+            v[r] = make_float2(a, has_b ? b : 0.f);
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < PL::E; ++r) {
+            const long long s = s0 + t + PL::T * r;
+            const bool in = active && s >= 0 && s < n;
+            v[r] = make_float2(in ? __ldcs(&xa[s]) : 0.f, (in && has_b) ? __ldcs(&xb[s]) : 0.f);
+        }
     }
     fft_block<PL, -1, 1>(v, smg, t, tw);
 #pragma unroll
@@ -70,6 +83,19 @@ fir_fft_kernel(const float* __restrict__ x, int lines, int n, int nb, const floa
     if (!active) return;
     float* ya = y + (size_t)la * n;
     float* yb = y + (size_t)lb * n;
+    // every output of an interior block exists and none lies within the zi history
+    if (s0 >= 0 && out0 + step <= n) {
+        float* qa = ya + s0 + t;
+        float* qb = yb + s0 + t;
+#pragma unroll
+        for (int r = 0; r < PL::E; ++r) {
+            if (t + PL::T * r >= hist) {
+                qa[PL::T * r] = v[r].x;  // stays in L2 for the next stage
+                if (has_b) qb[PL::T * r] = v[r].y;
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int r = 0; r < PL::E; ++r) {
         const int e = t + PL::T * r;
