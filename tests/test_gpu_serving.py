@@ -110,12 +110,18 @@ def test_host_and_device_inputs_in_one_batch(z):
     P, N = 64, 2048
     cpis = [make_cpi(P, N, 8, 128, seed=500 + i) for i in range(8)]
     rep = torch.as_tensor(cpis[0].replica).cuda()
+    # every buffer exists before the first submit, so the requests arrive back to back
+    # and queue behind the first batch instead of trickling in one per completion
+    bufs = []
+    for i, c in enumerate(cpis):
+        x = torch.as_tensor(c.x).pin_memory() if i % 2 else torch.as_tensor(c.x).cuda()
+        det = torch.empty((P, N), dtype=torch.uint8).pin_memory()
+        thr = torch.empty((P, N), dtype=torch.float32, device="cuda")
+        bufs.append((x, det, thr))
+    torch.cuda.synchronize()
     with z.RdServer(z.ServerConfig(max_batch=8)) as server:
         tickets = []
-        for i, c in enumerate(cpis):
-            x = torch.as_tensor(c.x).pin_memory() if i % 2 else torch.as_tensor(c.x).cuda()
-            det = torch.empty((P, N), dtype=torch.uint8).pin_memory()
-            thr = torch.empty((P, N), dtype=torch.float32, device="cuda")
+        for x, det, thr in bufs:
             tickets.append((server.submit(x, rep, 3, det, threshold=thr), det, thr))
         for t, _, _ in tickets:
             server.wait(t)

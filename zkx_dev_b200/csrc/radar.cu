@@ -322,6 +322,13 @@ pulse_doppler_tma_kernel(const __grid_constant__ CUtensorMap tmap, int pulses, i
         for (int b = 0; b < N / BOXH; ++b)
             tma_load_2d(sm + b * BOXH * C, &tmap, 2 * col0, cpi * pulses + b * BOXH, bar);
     }
+    // the window weights arrive while the tile is in flight
+    float wv[PL::E];
+#pragma unroll
+    for (int r = 0; r < PL::E; ++r) {
+        const int e = t + PL::T * r;
+        wv[r] = (window && e < pulses) ? __ldg(&window[e]) : 1.f;
+    }
     const bool ok = mbar_wait_bounded(bar, 0);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
@@ -336,9 +343,8 @@ pulse_doppler_tma_kernel(const __grid_constant__ CUtensorMap tmap, int pulses, i
         // rows past this CPI's pulses (zero padding to nfft) may hold the next CPI's data
         float2 a = e < pulses ? sm[e * C + c] : make_float2(0.f, 0.f);
         if (window && e < pulses) {
-            const float w = __ldg(&window[e]);
-            a.x *= w;
-            a.y *= w;
+            a.x *= wv[r];
+            a.y *= wv[r];
         }
         v[r] = a;
     }
