@@ -261,6 +261,42 @@ __device__ __forceinline__ void apply_twiddles(float2* v, int n, const float2* _
     }
 }
 
+// The LOGR table entries apply_twiddles reads (W_Mprev^(n p), p = 1, 2, 4, ...), for
+// callers that issue these loads early, e.g. while a tile copy is still in flight.
+template <int R, int LOGMPREV>
+__device__ __forceinline__ void load_twiddle_bases(float2 (&wb)[ilog2(R) > 0 ? ilog2(R) : 1], int n,
+                                                   const float2* __restrict__ tw)
+{
+    const unsigned base = (unsigned)n << (kTwiddleLog - LOGMPREV);
+    static_for<0, ilog2(R)>([&](auto B) {
+        constexpr int b = decltype(B)::value;
+        wb[b] = __ldg(&tw[(base << b) & (kTwiddleSize - 1)]);
+    });
+}
+
+// apply_twiddles from bases loaded by load_twiddle_bases (the same products, in the
+// same order, so the results are bit-identical).
+template <int R, int DIR>
+__device__ __forceinline__ void apply_twiddles_from(float2* v, const float2* wb)
+{
+    if constexpr (R > 1) {
+        constexpr int LOGR = ilog2(R);
+        float2 w[R];
+        static_for<0, LOGR>([&](auto B) {
+            constexpr int b = decltype(B)::value;
+            w[1 << b] = DIR > 0 ? cconj(wb[b]) : wb[b];
+        });
+        static_for<3, R>([&](auto K) {
+            constexpr int k = decltype(K)::value;
+            if constexpr ((k & (k - 1)) != 0) {
+                constexpr int hi = 1 << ilog2(k);
+                w[k] = cmul(w[hi], w[k - hi]);
+            }
+        });
+        static_for<1, R>([&](auto K) { v[decltype(K)::value] = cmul(v[decltype(K)::value], w[decltype(K)::value]); });
+    }
+}
+
 // The same product with W_Mprev^(n k) read from a per-CTA shared table tab[n (R + 1) + k]
 // (n < M of the pass; the odd row pitch keeps the lanes' reads on distinct banks).
 template <int R, int DIR>
@@ -298,7 +334,8 @@ __device__ __forceinline__ void fill_mid_table(float2* tab, int t, int nthreads,
 // must call this (it synchronises the block).
 template <class PL, int DIR, int C, bool PAD = true>
 __device__ __forceinline__ void fft_block(float2 (&v)[PL::E], float2* sm, int t,
-                                          const float2* __restrict__ tw, const float2* mid = nullptr)
+                                          const float2* __restrict__ tw, const float2* mid = nullptr,
+                                          const float2* first = nullptr)
 {
     constexpr int E = PL::E;
     constexpr int T = PL::T;
@@ -306,9 +343,13 @@ __device__ __forceinline__ void fft_block(float2 (&v)[PL::E], float2* sm, int t,
         dft<E, DIR>(v);
         return;
     } else {
-        // pass 1: n = t, s = 0, radix E, twiddle W_N^(t k)
+        // pass 1: n = t, s = 0, radix E, twiddle W_N^(t k) (bases preloaded in `first`
+        // by load_twiddle_bases<E, PL::LOGN>(first, t, tw) when the caller has them)
         dft<E, DIR>(v);
-        apply_twiddles<E, DIR, PL::LOGN>(v, t, tw);
+        if (first != nullptr)
+            apply_twiddles_from<E, DIR>(v, first);
+        else
+            apply_twiddles<E, DIR, PL::LOGN>(v, t, tw);
         static_for<0, E>([&](auto K) {
             constexpr int k = decltype(K)::value;
             sm[padded<PL, 1, PAD>(k * PL::M(1) + t) * C] = v[k];

@@ -322,13 +322,16 @@ pulse_doppler_tma_kernel(const __grid_constant__ CUtensorMap tmap, int pulses, i
         for (int b = 0; b < N / BOXH; ++b)
             tma_load_2d(sm + b * BOXH * C, &tmap, 2 * col0, cpi * pulses + b * BOXH, bar);
     }
-    // the window weights arrive while the tile is in flight
+    // the window weights and the first pass's twiddle bases arrive while the tile is
+    // in flight
     float wv[PL::E];
 #pragma unroll
     for (int r = 0; r < PL::E; ++r) {
         const int e = t + PL::T * r;
         wv[r] = (window && e < pulses) ? __ldg(&window[e]) : 1.f;
     }
+    float2 wb[ilog2(PL::E) > 0 ? ilog2(PL::E) : 1];
+    if constexpr (PL::PASSES > 1) load_twiddle_bases<PL::E, PL::LOGN>(wb, t, tw);
     const bool ok = mbar_wait_bounded(bar, 0);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
@@ -349,7 +352,7 @@ pulse_doppler_tma_kernel(const __grid_constant__ CUtensorMap tmap, int pulses, i
         v[r] = a;
     }
     __syncthreads();
-    fft_block<PL, -1, C, (C < 16)>(v, sm + c, t, tw);
+    fft_block<PL, -1, C, (C < 16)>(v, sm + c, t, tw, nullptr, PL::PASSES > 1 ? wb : nullptr);
     if (active) {
 #pragma unroll
         for (int r = 0; r < PL::E; ++r) {
