@@ -139,6 +139,17 @@ pulse_compression_persistent_kernel(const Src src, int pulses, int samples,
     float2* mid = mid_table_elems<PL>() > 0 ? sm + PL::smem_elems() + 2 : nullptr;
     const int t = threadIdx.x;
     if (mid) fill_mid_table<PL>(mid, t, PL::T, tw);
+    // first-pass twiddle bases, the same for every pulse and both directions: each
+    // thread keeps its own in shared memory at an odd pitch of float2 (the 64-bit reads
+    // of 16 lanes then land on distinct bank pairs)
+    constexpr int LOGE = ilog2(PL::E);
+    float2* first = sm + PL::smem_elems() + 2 + mid_table_elems<PL>() + t * (LOGE | 1);
+    {
+        float2 wb[LOGE];
+        load_twiddle_bases<PL::E, PL::LOGN>(wb, t, tw);
+#pragma unroll
+        for (int b = 0; b < LOGE; ++b) first[b] = wb[b];
+    }
     const int copy = samples < N ? samples : N;                 // elements staged per pulse
     const uint32_t bytes = (uint32_t)copy * (uint32_t)sizeof(float2);
     constexpr uint32_t kChunk = 32768;                          // bytes per bulk copy
@@ -175,11 +186,11 @@ pulse_compression_persistent_kernel(const Src src, int pulses, int samples,
             v[r] = e < copy ? sm[e] : make_float2(0.f, 0.f);
         }
         __syncthreads();
-        fft_block<PL, -1, 1>(v, sm, t, tw, mid);
+        fft_block<PL, -1, 1>(v, sm, t, tw, mid, first);
 #pragma unroll
         for (int r = 0; r < PL::E; ++r) v[r] = cmul(v[r], __ldg(&spectrum[t + PL::T * r]));
         __syncthreads();
-        fft_block<PL, 1, 1>(v, sm, t, tw, mid);
+        fft_block<PL, 1, 1>(v, sm, t, tw, mid, first);
         // every thread is done with the exchange buffer; order those accesses before the
         // bulk copy that overwrites it
         fence_proxy_async_smem();
@@ -399,7 +410,8 @@ int compression_impl(const Src& x, bool aligned16, int pulses, int samples, cons
             int dev = 0, sms = 0;
             ZKX_CUDA(cudaGetDevice(&dev));
             ZKX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            const size_t smem = ((size_t)PL::smem_elems() + 2 + mid_table_elems<PL>()) * sizeof(float2);
+            const size_t smem = ((size_t)PL::smem_elems() + 2 + mid_table_elems<PL>() +
+                                 (size_t)PL::T * (ilog2(PL::E) | 1)) * sizeof(float2);
             auto k = pulse_compression_persistent_kernel<N, Src>;
             ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             int per_sm = 0;
