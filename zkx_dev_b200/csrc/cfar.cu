@@ -271,7 +271,9 @@ cfar_accurate_tma_kernel(const __grid_constant__ CUtensorMap tmap, int rows, int
         return;
     }
 
-    constexpr int SEG = 16;
+    // 32-row segments: the vertical pass of a 64 x 64 tile is one round of the CTA's threads
+    // (84 halo columns x 2 segments for the 2/8 window) and sums fewer halo rows per cell
+    constexpr int SEG = 32;
     constexpr int VL = SEG + 2 * MR;
     for (int item = threadIdx.x; item < HC * (TY / SEG); item += kCfarThreads) {
         const int seg = item / HC;
