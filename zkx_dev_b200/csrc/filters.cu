@@ -22,9 +22,10 @@ namespace {
 
 constexpr int kFirThreads = 256;
 // From this many taps the overlap-save FFT path (firfft.cu) beats the direct sums: on
-// 16 x 2^20 samples 63 taps take 82 us direct and 96 us by FFT, 95 taps 100 and 96 us,
-// 127 taps 117 and 92 us (the FFT path stays near 92 us up to 511 taps).
-constexpr int kFirFftMinTaps = 80;
+// 16 x 2^20 samples 15 taps take 48.0 us direct and 49.4 us by FFT, 31 taps 55.2 and 49.5,
+// 63 taps 70.4 and 51.4, 127 taps 106.4 and 51.4 (the FFT path stays within 48-72 us up
+// to 511 taps).
+constexpr int kFirFftMinTaps = 20;
 constexpr int kFirPerThread = 16;
 constexpr int kFirBlock = kFirThreads * kFirPerThread;  // outputs per CTA
 
