@@ -243,12 +243,25 @@ firfilter2_fft_kernel(const float* __restrict__ x, int lines, int n, int nb, int
     const float* xa = x + (size_t)la * n;
     const float* xb = x + (size_t)(has_b ? lb : la) * n;
     float2 v[PL::E];
+    if (active && s0 >= edge && s0 + N <= (long long)edge + n) {
+        // a block wholly inside the line: extended sample i is x[i - edge], read at
+        // constant offsets without the padding logic
+        const float* pa = xa + (s0 - edge) + t;
+        const float* pb = xb + (s0 - edge) + t;
 #pragma unroll
-    for (int r = 0; r < PL::E; ++r) {
-        const long long i = s0 + t + PL::T * r;
-        const bool in = active && i < ne;
-        v[r] = make_float2(in ? extended_sample(xa, n, edge, padtype, rounding, i) : 0.f,
-                           (in && has_b) ? extended_sample(xb, n, edge, padtype, rounding, i) : 0.f);
+        for (int r = 0; r < PL::E; ++r) {
+            const float a = __ldcs(pa + PL::T * r);
+            const float b = __ldcs(pb + PL::T * r);
+            v[r] = make_float2(a, has_b ? b : 0.f);
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < PL::E; ++r) {
+            const long long i = s0 + t + PL::T * r;
+            const bool in = active && i < ne;
+            v[r] = make_float2(in ? extended_sample(xa, n, edge, padtype, rounding, i) : 0.f,
+                               (in && has_b) ? extended_sample(xb, n, edge, padtype, rounding, i) : 0.f);
+        }
     }
     fft_block<PL, -1, 1>(v, smg, t, tw);
 #pragma unroll
@@ -261,6 +274,20 @@ firfilter2_fft_kernel(const float* __restrict__ x, int lines, int n, int nb, int
     if (!active) return;
     float* ya = y + (size_t)la * n;
     float* yb = y + (size_t)lb * n;
+    if (out0 + step <= n) {
+        // every output of the block exists: store at constant offsets from the first
+        float* qa = ya + out0 - hist + t;
+        float* qb = yb + out0 - hist + t;
+#pragma unroll
+        for (int r = 0; r < PL::E; ++r) {
+            const int e = t + PL::T * r;
+            if (e >= hist && e < hist + step) {
+                __stcs(qa + PL::T * r, v[r].x);
+                if (has_b) __stcs(qb + PL::T * r, v[r].y);
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int r = 0; r < PL::E; ++r) {
         const int e = t + PL::T * r;
