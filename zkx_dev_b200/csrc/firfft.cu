@@ -35,8 +35,20 @@ fir_spectrum_kernel(const float* __restrict__ b, int nb, float2* __restrict__ H,
     for (int r = 0; r < PL::E; ++r) H[t + PL::T * r] = v[r];
 }
 
+// CTAs per SM the register budget is sized for: four 128-thread CTAs for 1024 points (128
+// registers, 47.5 us against 51.5 us with three at 168 registers and 53.6 us with five,
+// which spill; 127 taps on 16 x 2^20); two for the other 32-value plans (three would cap
+// them at 80 registers and spill); three of up to 256 threads otherwise.
 template <int N, int G>
-__global__ void __launch_bounds__(G * FftPlan<N, elems_for(N)>::T, G * FftPlan<N, elems_for(N)>::T <= 256 ? 3 : 1)
+constexpr int fir_fft_min_blocks()
+{
+    return N == 1024 ? 4
+         : G * FftPlan<N, elems_for(N)>::T > 256 ? 1
+         : elems_for(N) >= 32 ? 2 : 3;
+}
+
+template <int N, int G>
+__global__ void __launch_bounds__(G * FftPlan<N, elems_for(N)>::T, (fir_fft_min_blocks<N, G>()))
 fir_fft_kernel(const float* __restrict__ x, int lines, int n, int nb, const float2* __restrict__ H,
                const float* __restrict__ zi, float* __restrict__ y, const float2* __restrict__ tw)
 {
