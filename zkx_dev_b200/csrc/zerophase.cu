@@ -222,8 +222,16 @@ autocorr_spectrum_kernel(const float* __restrict__ b, int nb, float2* __restrict
         P[t + PL::T * r] = make_float2(fmaf(v[r].x, v[r].x, v[r].y * v[r].y) * inv, 0.f);
 }
 
+// Three CTAs of up to 256 threads per SM, two for the 32-value plans (three would cap them
+// at 80 registers and spill), one above 256 threads.
 template <int N, int G>
-__global__ void __launch_bounds__(G * FftPlan<N, elems_for(N)>::T, G * FftPlan<N, elems_for(N)>::T <= 256 ? 3 : 1)
+constexpr int zp_fft_min_blocks()
+{
+    return G * FftPlan<N, elems_for(N)>::T > 256 ? 1 : elems_for(N) >= 32 ? 2 : 3;
+}
+
+template <int N, int G>
+__global__ void __launch_bounds__(G * FftPlan<N, elems_for(N)>::T, (zp_fft_min_blocks<N, G>()))
 firfilter2_fft_kernel(const float* __restrict__ x, int lines, int n, int nb, int edge, int padtype, int rounding,
                       const float2* __restrict__ P, float* __restrict__ y, const float2* __restrict__ tw)
 {
