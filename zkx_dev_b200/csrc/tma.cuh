@@ -75,8 +75,6 @@ __device__ __forceinline__ void bulk_load_1d(void* dst, const void* src, uint32_
         : "memory");
 }
 
-// Orders this thread's earlier generic-proxy shared-memory accesses before later
-// async-proxy (bulk copy) writes to the same memory.
 // Asynchronous prefetch of [src, src + bytes) from global memory into L2 (no completion
 // signal; src 16-byte aligned, bytes a multiple of 16).
 __device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes)
@@ -84,6 +82,8 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
+// Orders this thread's earlier generic-proxy shared-memory accesses before later
+// async-proxy (bulk copy) writes to the same memory.
 __device__ __forceinline__ void fence_proxy_async_smem()
 {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
