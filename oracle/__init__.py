@@ -74,6 +74,7 @@ def restatement() -> ctypes.CDLL:
         lib.or_cfar_reference_count_2d.argtypes = [_I, _I, _I, _I]
         lib.or_ca_cfar_compat_f32.argtypes = [_P, _I, _I, _I, _I, _I, _I, _I, _D, _P, _P]
         lib.or_ca_cfar_f64.argtypes = [_P, _I, _I, _I, _I, _I, _I, _D, _P, _P]
+        lib.or_ca_cfar_f64_rows.argtypes = [_P, _I, _I, _I, _I, _I, _I, _D, _I, _I, _P, _P]
         lib.or_firfilter.argtypes = [_P, _I, _P, _I, _I, _P, _P, _P]
         lib.or_upfirdn_length.restype = ctypes.c_int64
         lib.or_upfirdn_length.argtypes = [_I, _I, _I, _I]
@@ -280,6 +281,33 @@ def ca_cfar_f64(x, guard, train, pfa: float):
     _check(restatement().or_ca_cfar_f64(
         x.ctypes.data, rows, cols, guard[0], guard[1], train[0], train[1], pfa,
         thr.ctypes.data, det.ctypes.data))
+    return thr, det
+
+
+def ca_cfar_f64_bands(x, guard, train, pfa: float, threads: Optional[int] = None,
+                      band_rows: int = 64):
+    """The FP64 truth CA-CFAR of ``ca_cfar_f64`` computed separably in row bands on
+    several threads (``or_ca_cfar_f64_rows``; ctypes releases the GIL during each call),
+    for full planes of 10^7-10^8 cells.  Returns (threshold64, mask)."""
+    import concurrent.futures as cf
+    x = _f32(x)
+    rows, cols = x.shape
+    thr = np.zeros(x.shape, dtype=np.float64)
+    det = np.zeros(x.shape, dtype=np.uint8)
+    lib = restatement()
+    if threads is None:
+        threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+    def band(r0: int) -> int:
+        r1 = min(rows, r0 + band_rows)
+        return lib.or_ca_cfar_f64_rows(x.ctypes.data, rows, cols, guard[0], guard[1], train[0],
+                                       train[1], pfa, r0, r1,
+                                       thr.ctypes.data + r0 * cols * 8,
+                                       det.ctypes.data + r0 * cols)
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
+        for rc in ex.map(band, range(0, rows, band_rows)):
+            _check(rc)
     return thr, det
 
 

@@ -339,6 +339,61 @@ int or_ca_cfar_f64(const float* x, int rows, int columns, int gr, int gc, int rr
     return OR_OK;
 }
 
+int or_ca_cfar_f64_rows(const float* x, int rows, int columns, int gr, int gc, int rr, int rc,
+                        double pfa, int row_begin, int row_end, double* threshold64,
+                        uint8_t* detections)
+{
+    /* Same geometry, border rule and test as or_ca_cfar_f64 (rt.cpp:161-220,465-555). */
+    if (!validate_cfar(2, rows, columns, gr, gc, rr, rc, pfa)) return OR_INVALID;
+    if (row_begin < 0 || row_end > rows || row_begin > row_end) return OR_INVALID;
+    const int count_ref = or_cfar_reference_count_2d(gr, gc, rr, rc);
+    double alpha;
+    or_cfar_alpha(pfa, count_ref, &alpha);
+    const double scale = alpha / (double)count_ref;
+    const int rm = gr + rr, cm = gc + rc;
+    const int in_lo = row_begin - rm < 0 ? 0 : row_begin - rm;
+    const int in_hi = row_end + rm > rows ? rows : row_end + rm;
+    const int band = in_hi - in_lo;
+    /* full[r][c]: sum over |dc| <= cm; side[r][c]: sum over gc < |dc| <= cm */
+    double* full = (double*)calloc((size_t)band * columns, sizeof(double));
+    double* side = (double*)calloc((size_t)band * columns, sizeof(double));
+    if (band > 0 && (!full || !side)) { free(full); free(side); return OR_INVALID; }
+    for (int r = in_lo; r < in_hi; ++r) {
+        const float* xr = x + (size_t)r * columns;
+        double* fr = full + (size_t)(r - in_lo) * columns;
+        double* sr = side + (size_t)(r - in_lo) * columns;
+        for (int c = cm; c < columns - cm; ++c) {
+            double s = 0.0;
+            for (int dc = -cm; dc < -gc; ++dc) s += (double)xr[c + dc];
+            for (int dc = gc + 1; dc <= cm; ++dc) s += (double)xr[c + dc];
+            double f = s;
+            for (int dc = -gc; dc <= gc; ++dc) f += (double)xr[c + dc];
+            fr[c] = f;
+            sr[c] = s;
+        }
+    }
+    for (int r = row_begin; r < row_end; ++r) {
+        const size_t o = (size_t)(r - row_begin) * columns;
+        const int interior_row = r >= rm && r < rows - rm;
+        for (int c = 0; c < columns; ++c) {
+            double t = 0.0;
+            if (interior_row && c >= cm && c < columns - cm) {
+                double sum = 0.0;
+                for (int dr = -rm; dr <= rm; ++dr) {
+                    const size_t k = (size_t)(r + dr - in_lo) * columns + c;
+                    sum += (dr < -gr || dr > gr) ? full[k] : side[k];
+                }
+                t = scale * sum;
+            }
+            if (threshold64) threshold64[o + c] = t;
+            detections[o + c] = ((double)x[(size_t)r * columns + c] > t) ? 1 : 0;
+        }
+    }
+    free(full);
+    free(side);
+    return OR_OK;
+}
+
 /* ------------------------------------------------------------------ filters */
 
 int or_firfilter(const float* b, int nb, const float* x, int rows, int n, const float* zi,

@@ -74,6 +74,21 @@ int or_ca_cfar_f64(const float* x, int rows, int columns,
                    int reference_rows, int reference_columns, double pfa,
                    double* threshold64, uint8_t* detections);
 
+/* The same FP64 truth for output rows [row_begin, row_end) only, with the ring sum
+ * taken separably: per input row, the full-width and the two side-band column sums
+ * (each a direct FP64 sum of its cells), then the ring = sum of full-width sums over
+ * the training rows + sum of side-band sums over the guard rows.  Every term is an
+ * input cell (no difference of partial sums), so for a power plane no cancellation
+ * enters; the result equals
+ * or_ca_cfar_f64 up to FP64 summation order.  threshold64 / detections point at the
+ * band's first output row ([row_end - row_begin, columns]); bands are independent, so
+ * callers may compute them on several threads at once. */
+int or_ca_cfar_f64_rows(const float* x, int rows, int columns,
+                        int guard_rows, int guard_columns,
+                        int reference_rows, int reference_columns, double pfa,
+                        int row_begin, int row_end,
+                        double* threshold64, uint8_t* detections);
+
 /* firfilter along the last axis of [rows, n] (ft.cpp:1536-1590): double
  * accumulation in tap order, rounded to float.  zi/zf are [rows, nb-1] or NULL. */
 int or_firfilter(const float* b, int nb, const float* x, int rows, int n,
