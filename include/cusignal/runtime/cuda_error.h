@@ -1,5 +1,6 @@
 // CUDA_CHECK: throws ProjectError{CUDA_RUNTIME_ERROR or OUT_OF_MEMORY} on a failing CUDA
-// runtime call (the contract of ZKX/cusignal_cpp/include/cusignal/runtime/cuda_error.h:5-56).
+// runtime call; CUDA_KERNEL_CHECK(): the same for the error a kernel launch left behind
+// (the contract of ZKX/cusignal_cpp/include/cusignal/runtime/cuda_error.h:5-56).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -18,7 +19,18 @@ namespace cusignal::cuda_utils {
                                  ": " + cudaGetErrorString(status));
 }
 
+// Launch-time error of the last kernel launch on this thread (bad configuration, no
+// device image), as CUDA_CHECK reports it; asynchronous faults surface at the next
+// synchronising call instead.
+inline void check_last_kernel_error(const char* file, int line)
+{
+    const cudaError_t status = cudaGetLastError();
+    if (status != cudaSuccess) throw_cuda_error(status, "kernel launch", file, line);
+}
+
 }  // namespace cusignal::cuda_utils
+
+#define CUDA_KERNEL_CHECK() ::cusignal::cuda_utils::check_last_kernel_error(__FILE__, __LINE__)
 
 #define CUDA_CHECK(call)                                                                     \
     do {                                                                                     \

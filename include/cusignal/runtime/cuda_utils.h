@@ -1,12 +1,15 @@
 // Host helpers of the cusignal_cpp runtime that callers use around the operators
-// (ZKX/cusignal_cpp/include/cusignal/runtime/copy_utils.h, runtime_utils.h): copies on a
-// stream, a default-stream synchronisation and the device memory counters.
+// (ZKX/cusignal_cpp/include/cusignal/runtime/cuda_utils.h, copy_utils.h): copies on a
+// stream and a default-stream synchronisation, plus the device queries and event timer
+// (runtime_utils.h) and the 1-D launch helpers (kernel_launch.h) it gathers.
 #pragma once
 
 #include <cuda_runtime.h>
 
 #include <cusignal/runtime/cuda_error.h>
 #include <cusignal/runtime/device_array.h>
+#include <cusignal/runtime/kernel_launch.h>
+#include <cusignal/runtime/runtime_utils.h>
 
 #include <cstddef>
 
@@ -31,17 +34,5 @@ inline void copy_device_to_device(T* dst, const T* src, std::size_t count, cudaS
 }
 
 inline void synchronize_stream(cudaStream_t stream = nullptr) { CUDA_CHECK(cudaStreamSynchronize(stream)); }
-
-struct MemoryInfo {
-    std::size_t free_bytes = 0;
-    std::size_t total_bytes = 0;
-};
-
-inline MemoryInfo current_memory_info()
-{
-    MemoryInfo m;
-    CUDA_CHECK(cudaMemGetInfo(&m.free_bytes, &m.total_bytes));
-    return m;
-}
 
 }  // namespace cusignal::cuda_utils

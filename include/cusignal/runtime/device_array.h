@@ -1,11 +1,14 @@
 // DeviceArray<T>: move-only owner of a cudaMalloc'd array with explicit host transfers,
 // the container of the cusignal_cpp API (ZKX/cusignal_cpp/include/cusignal/runtime/
 // device_array.h:19-121).  from_host/to_host copy on the legacy default stream and wait.
+// Allocations go through the tracked allocator (device_allocation_tracker.h), so
+// tracked_device_current_bytes / tracked_device_peak_bytes cover every array.
 #pragma once
 
 #include <cuda_runtime.h>
 
 #include <cusignal/runtime/cuda_error.h>
+#include <cusignal/runtime/device_allocation_tracker.h>
 
 #include <cstddef>
 #include <vector>
@@ -62,7 +65,7 @@ public:
     void reset()
     {
         if (data_) {
-            const cudaError_t st = cudaFree(data_);
+            const cudaError_t st = cuda_utils::tracked_cuda_free(data_);
             data_ = nullptr;
             size_ = 0;
             CUDA_CHECK(st);
@@ -80,13 +83,13 @@ private:
     {
         reset();
         if (count == 0) return;
-        CUDA_CHECK(cudaMalloc(reinterpret_cast<void**>(&data_), count * sizeof(T)));
+        CUDA_CHECK(cuda_utils::tracked_cuda_malloc(&data_, count * sizeof(T)));
         size_ = count;
     }
     void release() noexcept
     {
         if (data_) {
-            (void)cudaFree(data_);
+            (void)cuda_utils::tracked_cuda_free(data_);
             data_ = nullptr;
             size_ = 0;
         }

@@ -38,8 +38,18 @@ def build_restatement() -> None:
     subprocess.run(["make", "-s", "-C", _HERE, "restatement"], check=True)
 
 
-def build_reference(ref_root: str = "/root/reference") -> bool:
+def reference_root() -> str:
+    """The ZKX_dev checkout the reference builds read: $ZKX_REFERENCE_ROOT when set, else a
+    checkout named "reference" beside this repository."""
+    env = os.environ.get("ZKX_REFERENCE_ROOT")
+    if env:
+        return env
+    return os.path.normpath(os.path.join(_HERE, "..", "..", "reference"))
+
+
+def build_reference(ref_root: Optional[str] = None) -> bool:
     """Compile the reference CPU library when the reference checkout is present."""
+    ref_root = ref_root or reference_root()
     if not os.path.isdir(os.path.join(ref_root, "ZKX", "cusignal_cpp")):
         return False
     subprocess.run(["make", "-s", "-j8", "-C", _HERE, "ref", f"REF_ROOT={ref_root}"],
@@ -47,12 +57,23 @@ def build_reference(ref_root: str = "/root/reference") -> bool:
     return True
 
 
-def build_probes(ref_root: str = "/root/reference") -> bool:
+def build_probes(ref_root: Optional[str] = None) -> bool:
     """Compile the reference's own operator probes against include/ and libzkx_rd.so
     (test infrastructure for the drop-in check) when the reference checkout is present."""
+    ref_root = ref_root or reference_root()
     if not os.path.isdir(os.path.join(ref_root, "ZKX", "test_all")):
         return False
     subprocess.run(["make", "-s", "-j8", "-C", _HERE, "probes", f"REF_ROOT={ref_root}"], check=True)
+    return True
+
+
+def build_task1(ref_root: Optional[str] = None) -> bool:
+    """Compile the reference's Task1 pipeline and its pipeline benchmark, unchanged, against
+    include/ and libzkx_rd.so (the drop-in check for Task1) when the checkout is present."""
+    ref_root = ref_root or reference_root()
+    if not os.path.isdir(os.path.join(ref_root, "ZKX", "Task1", "pipeline")):
+        return False
+    subprocess.run(["make", "-s", "-j8", "-C", _HERE, "task1", f"REF_ROOT={ref_root}"], check=True)
     return True
 
 

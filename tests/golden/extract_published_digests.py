@@ -12,7 +12,10 @@ This script reads the archive in place (it needs the reference checkout) and wri
 ``published_digests.json`` beside itself; tests/test_oracle_published.py consumes that
 file without the reference.  Only FP32 cases are kept (the chain's arithmetic type).
 
-    python tests/golden/extract_published_digests.py [--ref /root/reference]
+    python tests/golden/extract_published_digests.py [--ref <ZKX_dev checkout>]
+
+The checkout defaults to $ZKX_REFERENCE_ROOT, else a checkout named "reference" beside
+this repository.
 """
 from __future__ import annotations
 
@@ -46,7 +49,9 @@ def parse_command(log_path: str) -> dict:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    here = os.path.dirname(os.path.abspath(__file__))
+    ap.add_argument("--ref", default=os.environ.get("ZKX_REFERENCE_ROOT")
+                    or os.path.normpath(os.path.join(here, "..", "..", "..", "reference")))
     opts = ap.parse_args()
     root = os.path.join(opts.ref, ARCHIVE)
     cases = {}

@@ -45,6 +45,31 @@ def test_dropin_headers_compile_and_link():
         assert os.path.exists(build_probe.build(d))
 
 
+def test_runtime_headers_host_side():
+    """The runtime headers Task1 and the probes include (errors, FP64 storage boundaries,
+    launch configuration) compile and behave on the host without a GPU."""
+    with tempfile.TemporaryDirectory() as d:
+        exe = build_probe.build(d, "runtime_probe")
+        r = subprocess.run([exe, "host"], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert "FAIL" not in r.stdout
+
+
+@pytest.mark.gpu
+def test_runtime_headers_on_device():
+    """Device queries, the event timer, 1-D launches with argument conversion to the
+    kernel's parameter types, device-side FP64 widening and the allocation tracker that
+    DeviceArray routes through."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    with tempfile.TemporaryDirectory() as d:
+        exe = build_probe.build(d, "runtime_probe")
+        r = subprocess.run([exe, "device"], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert "FAIL" not in r.stdout
+
+
 @pytest.mark.gpu
 def test_dropin_api_matches_oracle():
     torch = pytest.importorskip("torch")
