@@ -120,8 +120,10 @@ ZKX_API int zkx_pulse_compression_c64(const void* x, int num_pulses, int samples
  * as zkx_pulse_compression_c64 (the caller passes inputs and outputs); the replica
  * spectrum goes to a file-scope device array of 16384 complex64 (128 KiB) that every
  * GPU loading the library holds until the process exits.  nfft above 16384 is
- * rejected with ZKX_INVALID_ARGUMENT.  The first call on a device initialises the
- * library's twiddle table there (a synchronous set-up) and looks up the array's
+ * rejected with ZKX_INVALID_ARGUMENT, and an nfft that is not a power of two (with
+ * nfft = -1: a samples_per_pulse that is not one) with ZKX_UNSUPPORTED_OPERATION, since
+ * the chirp-z transform the allocating entry uses for those lengths needs a workspace.
+ * The first call on a device initialises the library's twiddle table there (a synchronous set-up) and looks up the array's
  * device address, so make that first call before any stream capture.  All calls share
  * the array: calls that overlap on the GPU (other streams or host threads) race.
  * No counterpart in the reference. */
@@ -457,8 +459,13 @@ ZKX_API int zkx_rd_graph_destroy(zkx_rd_graph graph);
  * device slots and the HBM budget allow, fuses pending CPIs of one shape and waveform
  * into one batched launch per stage, and spreads the batches over several CUDA
  * streams so copies and kernels of different batches overlap.  Replica spectra and
- * Doppler windows stay resident per (shape, waveform); per-batch workspaces come from
- * a stream-ordered memory pool and are counted against the budget. */
+ * Doppler windows stay resident per (shape, waveform).  Each batch runs in a workspace
+ * block the server owns: the smallest idle block that is large enough, else a new block
+ * (cudaMalloc, sizes rounded up to classes 2^k x {1, 1.25, 1.5, 1.75}) after idle blocks
+ * are freed to make room; a batch's completion callback returns its block to the idle
+ * list, and zkx_rd_server_destroy frees them all.  Every block held (in flight or idle)
+ * plus the resident plans stays within the HBM budget: a batch is admitted only when its
+ * block fits, so once the blocks of a stream's sizes exist nothing more is allocated. */
 
 /* Zero fields take the defaults named in the comments. */
 typedef struct {
@@ -501,7 +508,9 @@ typedef struct {
     double mean_batch;       /* CPIs per batch */
     double p50_us, p99_us, max_us, mean_us;  /* submit -> results in the caller's buffers */
     double cpis_per_s;       /* completed / (last completion - first submission) */
-    size_t budget_bytes, peak_bytes, plan_bytes;
+    size_t budget_bytes;
+    size_t peak_bytes;       /* most workspace-block bytes held at once (in flight + idle) */
+    size_t plan_bytes;       /* resident replica spectra and Doppler windows */
     int plans;
 } zkx_rd_server_stats;
 

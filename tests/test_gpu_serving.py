@@ -156,6 +156,31 @@ def test_admission_within_budget(z):
         assert torch.equal(det, alone(z, c, P, N)["detections"])
 
 
+def test_admission_tight_budget_counts_every_block(z):
+    """A budget only 5 % above one 128 x 4096 workspace: the block's size class (14 MB)
+    would not fit, so the server allocates the exact size; smaller CPIs of another shape
+    reuse that block.  Every block the server holds plus its plans stays within the budget
+    (peak_bytes counts idle blocks too), and every result equals the CPI processed alone."""
+    from zkx_dev_b200.synth import make_cpi
+    one = 2 * 128 * 4096 * 8 + 2 * 128 * 4096 * 4 + 128 * 4096 + 8 * 256
+    budget = int(1.05 * one)
+    reqs = [(128, 4096, make_cpi(128, 4096, 10, 256, seed=700 + i)) for i in range(4)]
+    reqs += [(64, 4096, make_cpi(64, 4096, 6, 256, seed=710 + i)) for i in range(4)]
+    with z.RdServer(z.ServerConfig(budget_bytes=budget, max_batch=8)) as server:
+        tickets = []
+        for P, N, c in reqs:
+            rep = torch.as_tensor(c.replica).cuda()
+            det = torch.empty((P, N), dtype=torch.uint8).pin_memory()
+            tickets.append((server.submit(torch.as_tensor(c.x).pin_memory(), rep, 11, det), det))
+        for t, _ in tickets:
+            server.wait(t)
+        st = server.stats()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    assert st["peak_bytes"] + st["plan_bytes"] <= budget
+    for (P, N, c), (_, det) in zip(reqs, tickets):
+        assert torch.equal(det, alone(z, c, P, N)["detections"])
+
+
 def test_oversized_request_is_refused(z):
     with z.RdServer(z.ServerConfig(budget_bytes=1 << 20)) as server:
         x = torch.zeros((64, 4096), dtype=torch.complex64)

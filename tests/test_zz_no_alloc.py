@@ -77,3 +77,12 @@ def test_noalloc_rejects_transforms_beyond_its_scratch(L):
     rc = L.lib().zkx_pulse_compression_c64_noalloc(p, 2, 32768, p, 8, -1, 1, 0, None, p, None)
     assert rc == L.INVALID_ARGUMENT
     assert b"16384" in L.lib().zkx_last_error()
+
+
+def test_noalloc_rejects_lengths_that_are_not_powers_of_two(L):
+    """The allocating entry point handles other lengths by the chirp-z transform, which
+    needs a workspace; this one refuses them (nfft = -1 takes the pulse length, 1000)."""
+    p = ctypes.c_void_p(16)
+    rc = L.lib().zkx_pulse_compression_c64_noalloc(p, 2, 1000, p, 8, -1, 1, 0, None, p, None)
+    assert rc == L.UNSUPPORTED_OPERATION
+    assert b"power of two" in L.lib().zkx_last_error()

@@ -276,13 +276,10 @@ int issue_batch(zkx_rd_server_s* s, const PlanEntry& pe, Batch* b, const Layout&
     return ZKX_SUCCESS;
 }
 
-// A workspace block of at least `need_bytes` for a batch admitted under the budget; called
-// by the worker with the lock held, which it drops around allocation and release calls.
-// The smallest idle block that is large enough is reused, so that after the first batches the
-// server holds about max_inflight blocks of the largest sizes and allocates nothing more (an
-// allocation of gigabytes in the middle of a stream stalls every request behind it);
-// otherwise idle blocks are released (largest first) until a new block of the size class fits
-// within the budget next to the blocks in use.
+// Workspace blocks.  The budget bounds every byte the server holds on the device: the blocks
+// of batches in flight (in_use), the idle blocks kept for reuse, and the resident plans, so
+// held + plan_bytes <= budget at all times (held = in_use + the idle blocks).
+//
 // Block sizes are rounded up to classes 2^k * {1, 1.25, 1.5, 1.75} (at least 1 MB), so that the
 // varying batch compositions of a request stream keep reusing a few blocks instead of
 // allocating new ones (an allocation can stall the device).
@@ -295,10 +292,32 @@ size_t size_class(size_t need)
     return base * 2;
 }
 
+// Bytes of the budget not taken by blocks in flight and plans (idle blocks can be released).
+size_t budget_room(const zkx_rd_server_s* s)
+{
+    const size_t taken = s->in_use + s->plan_bytes;
+    return s->budget > taken ? s->budget - taken : 0;
+}
+
+// Whether a batch whose workspace needs `need` bytes can have a block now within the budget:
+// an idle block large enough, or a new block once idle blocks are released.  Admission and
+// acquire_block use the same rule, so an admitted batch always gets its block.
+bool block_fits(const zkx_rd_server_s* s, size_t need)
+{
+    return s->idle.lower_bound(need) != s->idle.end() || need <= budget_room(s);
+}
+
+// A workspace block of at least `need_bytes` for a batch that block_fits admitted; called by
+// the worker with the lock held, which it drops around allocation and release calls.  The
+// smallest idle block that is large enough is reused, so that after the first batches the
+// server holds about max_inflight blocks of the largest sizes and allocates nothing more (an
+// allocation of gigabytes in the middle of a stream stalls every request behind it).
+// Otherwise idle blocks are released (largest first) until a new block fits within the
+// budget next to the blocks in flight; the new block takes its size class, or exactly
+// `need_bytes` when the class would not fit.
 int acquire_block(zkx_rd_server_s* s, std::unique_lock<std::mutex>& lk, size_t need_bytes, char** ws,
                   size_t* bytes)
 {
-    const size_t need = size_class(need_bytes);
     auto it = s->idle.lower_bound(need_bytes);
     if (it != s->idle.end()) {
         *ws = it->second;
@@ -306,6 +325,10 @@ int acquire_block(zkx_rd_server_s* s, std::unique_lock<std::mutex>& lk, size_t n
         s->idle.erase(it);
         return ZKX_SUCCESS;
     }
+    const size_t room = budget_room(s);
+    if (need_bytes > room) return fail(ZKX_OUT_OF_MEMORY, "serving: workspace exceeds the HBM budget");
+    const size_t cls = size_class(need_bytes);
+    const size_t need = cls <= room ? cls : need_bytes;
     std::vector<char*> release;
     while (s->held + need + s->plan_bytes > s->budget && !s->idle.empty()) {
         auto last = std::prev(s->idle.end());
@@ -314,6 +337,7 @@ int acquire_block(zkx_rd_server_s* s, std::unique_lock<std::mutex>& lk, size_t n
         s->idle.erase(last);
     }
     s->held += need;
+    s->peak = std::max(s->peak, s->held);
     lk.unlock();
     for (char* p : release) cudaFree(p);  // waits for the device; completions need the lock
     char* p = nullptr;
@@ -382,6 +406,19 @@ void worker_main(zkx_rd_server_s* s)
             }
             s->plan_bytes += (size_t)pe.range_bins * 8 + (size_t)pe.doppler_bins * 4;
             it = s->plans.emplace(head->key, pe).first;
+            // the plan's bytes count against the budget too: give back idle blocks if needed
+            std::vector<char*> release;
+            while (s->held + s->plan_bytes > s->budget && !s->idle.empty()) {
+                auto last = std::prev(s->idle.end());
+                s->held -= last->first;
+                release.push_back(last->second);
+                s->idle.erase(last);
+            }
+            if (!release.empty()) {
+                lk.unlock();
+                for (char* p : release) cudaFree(p);
+                lk.lock();
+            }
             continue;  // re-evaluate with the plan in place
         }
         const PlanEntry pe = it->second;
@@ -404,7 +441,7 @@ void worker_main(zkx_rd_server_s* s)
             const int st = staged + (q->x_on_device ? 0 : 1);
             const Layout trial = batch_layout(head->r.num_pulses, head->r.samples_per_pulse,
                                               (int)group.size() + 1, st, with_rd || q->r.rd, compat);
-            if (s->in_use + s->plan_bytes + trial.total > s->budget) break;
+            if (!block_fits(s, trial.total)) break;
             group.push_back(q);
             with_rd = with_rd || q->r.rd;
             staged = st;
@@ -434,7 +471,6 @@ void worker_main(zkx_rd_server_s* s)
             continue;
         }
         s->in_use += block_bytes;
-        s->peak = std::max(s->peak, s->in_use);
         ++s->next_stream;
         ++s->batches;
         s->batched_cpis += group.size();
@@ -668,6 +704,6 @@ extern "C" int zkx_rd_server_stats_reset(zkx_rd_server s)
     s->latency_us.clear();
     s->submitted = s->completed = s->failed = s->batches = s->batched_cpis = 0;
     s->have_first = false;
-    s->peak = s->in_use;
+    s->peak = s->held;
     return ZKX_SUCCESS;
 }
