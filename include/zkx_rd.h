@@ -123,9 +123,10 @@ ZKX_API int zkx_pulse_compression_c64(const void* x, int num_pulses, int samples
  * rejected with ZKX_INVALID_ARGUMENT, and an nfft that is not a power of two (with
  * nfft = -1: a samples_per_pulse that is not one) with ZKX_UNSUPPORTED_OPERATION, since
  * the chirp-z transform the allocating entry uses for those lengths needs a workspace.
- * The first call on a device initialises the library's twiddle table there (a synchronous set-up) and looks up the array's
- * device address, so make that first call before any stream capture.  All calls share
- * the array: calls that overlap on the GPU (other streams or host threads) race.
+ * The first call on a device initialises the library's twiddle table there (a
+ * synchronous set-up) and looks up the array's device address, so make that first call
+ * before any stream capture.  All calls share the array: calls that overlap on the GPU
+ * (other streams or host threads) race.
  * No counterpart in the reference. */
 ZKX_API int zkx_pulse_compression_c64_noalloc(const void* x, int num_pulses, int samples_per_pulse,
                                               const void* replica, int replica_length, int nfft,
