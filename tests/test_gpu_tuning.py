@@ -1,6 +1,8 @@
-"""The autotuner (zkx_rd_plan_autotune): every kernel choice it can make gives the same
-chain results bit for bit, the chosen values are valid, and later plans of the same shape
-start from them."""
+"""The autotuner (zkx_rd_plan_autotune): the kernel choices that share one transform
+(compression variants 1 and 2, both Doppler tile widths) give the same chain results bit
+for bit, variant 3 (its own four-step transform) agrees with the FP64 oracle and with them
+to FP32 rounding, the chosen values are valid, and later plans of the same shape start
+from them."""
 from __future__ import annotations
 
 import ctypes
@@ -50,10 +52,55 @@ def test_autotune_choice_is_valid_and_shared(z):
     rep = torch.as_tensor(lfm_chirp(L).astype(np.complex64)).cuda()
     chain = z.RangeDopplerChain(z.ChainConfig(P, N, L), rep)
     chosen = chain.autotune(x)
-    assert chosen["compression_variant"] in (1, 2) and chosen["doppler_columns"] in (8, 16)
+    assert chosen["compression_variant"] in (1, 2, 3) and chosen["doppler_columns"] in (8, 16)
     assert chain.tuning == chosen
     again = z.RangeDopplerChain(z.ChainConfig(P, N, L), rep)
     assert again.tuning == chosen
     out = again(x)
     torch.cuda.synchronize()
     assert out["detections"].sum().item() > 0
+
+
+@pytest.mark.parametrize("P,N,L,nfft", [(512, 8192, 512, -1), (1024, 4096, 256, -1), (128, 16384, 1024, -1),
+                                        (96, 3000, 200, 4096), (40, 20000, 1024, 16384)])
+def test_local_variant_matches_fp64(z, P, N, L, nfft):
+    """Variant 3 (the persistent kernel with the four-step transform and the spectrum held
+    in tensor memory) rounds differently from variants 1 and 2, so it is checked on its own:
+    compressed pulses against the FP64 oracle (zero padding and truncation included), within
+    FP32 rounding of variant 2, and a detection mask equal to the FP64 CFAR of its power."""
+    import oracle as O
+    from zkx_dev_b200.synth import make_cpi
+    cpi = make_cpi(P, N, 8, L, seed=P + N)
+    chain = z.RangeDopplerChain(z.ChainConfig(P, N, L, range_nfft=nfft), torch.as_tensor(cpi.replica).cuda())
+    x = torch.as_tensor(cpi.x).cuda()
+    set_tuning(chain, 2, 8)
+    ref = {k: v.clone() for k, v in chain(x).items()}
+    set_tuning(chain, 3, 8)
+    got = chain(x)
+    torch.cuda.synchronize()
+    comp = got["compressed"].cpu().numpy().astype(np.complex128)
+    comp2 = ref["compressed"].cpu().numpy().astype(np.complex128)
+    assert np.linalg.norm(comp - comp2) / np.linalg.norm(comp2) <= 1e-6
+    rows = [0, 1, P // 2, P - 1]
+    c64 = O.pulse_compression_fft64(cpi.x[rows], cpi.replica, nfft, True, O.radar_window_f32("hamming", L))
+    assert np.linalg.norm(comp[rows] - c64) / np.linalg.norm(c64) <= 1e-5
+    _, m64 = O.ca_cfar_f64(got["power"].cpu().numpy(), (2, 2), (8, 8), 1e-6)
+    np.testing.assert_array_equal(got["detections"].cpu().numpy(), m64)
+    from zkx_dev_b200 import _lib
+    assert _lib.kernel_status(clear=True) == 0
+
+
+def test_local_variant_stacked_batch(z):
+    """Variant 3 over a stack of CPIs (run_batch: one launch over all their pulses) gives
+    every CPI the result it gets alone."""
+    from zkx_dev_b200.synth import make_cpi
+    cpis = [make_cpi(64, 8192, 6, 512, seed=90 + b) for b in range(3)]
+    chain = z.RangeDopplerChain(z.ChainConfig(64, 8192, 512), torch.as_tensor(cpis[0].replica).cuda())
+    set_tuning(chain, 3, 8)
+    batch = chain.run_batch(torch.as_tensor(np.stack([c.x for c in cpis])).cuda())
+    torch.cuda.synchronize()
+    for b, c in enumerate(cpis):
+        alone = chain(torch.as_tensor(c.x).cuda())
+        torch.cuda.synchronize()
+        assert torch.equal(batch["compressed"][b], alone["compressed"])
+        assert torch.equal(batch["detections"][b], alone["detections"])

@@ -545,7 +545,11 @@ int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compresse
     if (!cumulative) cumulative = p->cumulative;
     if (p->d.cfar_mode == ZKX_CFAR_COMPAT && !cumulative)
         return fail(ZKX_INTERNAL_ERROR, "rd_execute: compat workspace missing");
-    // the CPIs of a batch are contiguous, so range compression sees batch*P pulses
+    // the CPIs of a batch are contiguous, so range compression sees batch*P pulses; the
+    // default kernel is chosen from one CPI's shape, so a CPI gets the same bits alone and in
+    // any batch
+    int variant = p->tuning.compression_variant;
+    ZKX_TRY(resolve_compression_variant(P, nr, variant, &variant));
     if (p->d.precision != ZKX_PRECISION_FP32) {
         if (table) return fail(ZKX_UNSUPPORTED_OPERATION, "rd_execute: tensor-core plans take contiguous batches");
         ZKX_TRY(launch_pulse_compression_tc(static_cast<const float2*>(x), batch * P, N, nr, p->spectrum,
@@ -553,11 +557,10 @@ int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compresse
     } else if (table)
         ZKX_TRY(launch_pulse_compression_table(reinterpret_cast<const float2* const*>(table), batch, P,
                                                N, nr, p->spectrum, static_cast<float2*>(compressed),
-                                               stream));
+                                               variant, stream));
     else
         ZKX_TRY(launch_pulse_compression_variant(static_cast<const float2*>(x), batch * P, N, nr, p->spectrum,
-                                                 static_cast<float2*>(compressed),
-                                                 p->tuning.compression_variant, stream));
+                                                 static_cast<float2*>(compressed), variant, stream));
     ZKX_TRY(launch_pulse_doppler(static_cast<const float2*>(compressed), P, nr, nd, p->doppler_window,
                                  static_cast<float2*>(rd), power, batch, p->tuning.doppler_columns, stream));
     const int* gd = p->d.guard_cells;
@@ -644,7 +647,7 @@ extern "C" int zkx_rd_plan_autotune(zkx_rd_plan p, const void* x, int batch, zkx
     int rc = ZKX_SUCCESS;
     if (p->d.precision == ZKX_PRECISION_FP32) {
         float tbest = 0.f;
-        for (int v : {ZKX_COMPRESSION_PLAIN, ZKX_COMPRESSION_PERSISTENT}) {
+        for (int v : {ZKX_COMPRESSION_PLAIN, ZKX_COMPRESSION_PERSISTENT, ZKX_COMPRESSION_LOCAL}) {
             float ms = 0.f;
             rc = time_median([&] {
                 return launch_pulse_compression_variant(static_cast<const float2*>(x), batch * P, N, nr,
@@ -693,7 +696,7 @@ extern "C" int zkx_rd_plan_get_tuning(zkx_rd_plan p, zkx_rd_tuning* t)
 extern "C" int zkx_rd_plan_set_tuning(zkx_rd_plan p, const zkx_rd_tuning* t)
 {
     if (!p || !t) return fail(ZKX_INVALID_ARGUMENT, "rd_plan_set_tuning: null pointer");
-    if (t->compression_variant < 0 || t->compression_variant > 2 ||
+    if (t->compression_variant < 0 || t->compression_variant > ZKX_COMPRESSION_LOCAL ||
         (t->doppler_columns != 0 && t->doppler_columns != 8 && t->doppler_columns != 16))
         return fail(ZKX_INVALID_ARGUMENT, "rd_plan_set_tuning: unknown kernel choice");
     p->tuning = *t;

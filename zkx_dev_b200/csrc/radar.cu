@@ -12,7 +12,9 @@
 #include <algorithm>
 
 #include "fft_core.cuh"
+#include "fft_local.cuh"
 #include "rows.cuh"
+#include "tcgen05.cuh"
 #include "tma.cuh"
 #include "window.cuh"
 #include "zkx_internal.h"
@@ -200,6 +202,149 @@ pulse_compression_persistent_kernel(const Src src, int pulses, int samples,
         float2* yr = y + (size_t)pulse * N;
 #pragma unroll
         for (int r = 0; r < PL::E; ++r) yr[t + PL::T * r] = v[r];  // stays in L2 for the next stage
+    }
+}
+
+// Persistent compression with the four-step ordering of fft_local.cuh (N = 4096, 8192,
+// 16384): the same pulse loop, bulk-copy staging, L2 prefetch and pass-1 twiddle bases as
+// the kernel above, but each direction synchronises the CTA twice instead of three or four
+// times.  The forward transform leaves each thread the spectrum bins of a fixed
+// digit-reversed set, so each thread writes its 2E spectrum words once, at the start, into
+// its own tensor-memory lane (tcgen05.st) and reads them back per pulse (tcgen05.ld): no
+// spectrum traffic from L2 per pulse (read at those bins from global memory, each warp
+// load would touch 16 sectors).  Warp w uses lanes 32 (w % 4) .. +31 and columns
+// (w / 4) 2E .. +2E-1 of the CTA's allocation, T / 128 * 2E columns: 256 at N = 16384
+// (one CTA per SM), 128 at 8192 (two), 64 at 4096 (four).  (Keeping the pass-1 twiddles
+// there as well, instead of forming them from bases, measured slower: 271.6 against
+// 265.8 us for the 1024 x 16384 chain.)
+template <int N>
+constexpr int local_tmem_columns()
+{
+    using LP = LocalPlan<N>;
+    constexpr int c = (LP::T / 128) * 2 * LP::E;
+    return c < 32 ? 32 : c;
+}
+
+// v[k] *= s_k (CONJ: conj(s_k)) with s_k the complex word pair at columns 2k, 2k+1.
+template <int E, bool CONJ>
+__device__ __forceinline__ void tmem_multiply(float2 (&v)[E], uint32_t cols)
+{
+#pragma unroll
+    for (int c = 0; c < 2 * E; c += 16) {
+        float w[16];
+        tmem_load16(cols + c, w);
+        tmem_wait_load();
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float2 m = make_float2(w[2 * i], w[2 * i + 1]);
+            v[c / 2 + i] = CONJ ? cmulc(v[c / 2 + i], m) : cmul(v[c / 2 + i], m);
+        }
+    }
+}
+
+template <int N, class Src>
+__global__ void __launch_bounds__(LocalPlan<N>::T)
+pulse_compression_local_kernel(const Src src, int pulses, int samples, const float2* __restrict__ spectrum,
+                               float2* __restrict__ y, const float2* __restrict__ tw, int* err)
+{
+    using LP = LocalPlan<N>;
+    constexpr int LOGE = ilog2(LP::E);
+    constexpr uint32_t kCols = local_tmem_columns<N>();
+    static_assert(LP::T % 128 == 0 && (2 * LP::E) % 16 == 0, "tensor-memory slice layout");
+    extern __shared__ __align__(128) float2 sm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + LP::EXCHANGE);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + LP::EXCHANGE + 1);
+    float2* tab = sm + LP::EXCHANGE + 2;
+    const int t = threadIdx.x;
+    const int warp = t >> 5;
+    if (warp == 0) {
+        tmem_alloc(tmem_slot, kCols);
+        tmem_relinquish();
+    }
+    // pass-2 twiddles and this thread's pass-1 twiddle bases, the same for every pulse
+    float2* first = tab + LP::TABLE + t * (LOGE | 1);
+    fill_local_table<LP>(tab, t, LP::T, tw);
+    {
+        float2 wb[LOGE];
+        load_twiddle_bases<LP::E, LP::LOGN>(wb, t, tw);
+#pragma unroll
+        for (int b = 0; b < LOGE; ++b) first[b] = wb[b];
+    }
+    if (t == 0) mbar_init(bar, 1);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const uint32_t spec_cols = tmem_base + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(warp >> 2) * (2 * LP::E);
+    // this thread's spectrum bins, in register order, into its tensor-memory lane
+#pragma unroll
+    for (int c = 0; c < 2 * LP::E; c += 16) {
+        float sv[16];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float2 b = __ldg(&spectrum[local_bin<LP>(t, c / 2 + i)]);
+            sv[2 * i] = b.x;
+            sv[2 * i + 1] = b.y;
+        }
+        tmem_store16(spec_cols + c, sv);
+    }
+    tmem_wait_store();
+    auto twiddle = [&](float2(&x)[LP::E]) { apply_twiddles_from<LP::E, -1>(x, first); };
+    auto twiddle_conj = [&](float2(&x)[LP::E]) { apply_twiddles_from<LP::E, 1>(x, first); };
+
+    const int copy = samples < N ? samples : N;
+    const uint32_t bytes = (uint32_t)copy * (uint32_t)sizeof(float2);
+    constexpr uint32_t kChunk = 32768;
+    auto issue = [&](int pulse) {
+        mbar_arrive_expect_tx(bar, bytes);
+        const char* from = reinterpret_cast<const char*>(src.row(pulse));
+        char* dst = reinterpret_cast<char*>(sm);
+        for (uint32_t off = 0; off < bytes; off += kChunk)
+            bulk_load_1d(dst + off, from + off, bytes - off < kChunk ? bytes - off : kChunk, bar);
+    };
+    int pulse = blockIdx.x;
+    if (t == 0 && pulse < pulses) issue(pulse);
+    uint32_t phase = 0;
+    bool timed_out = false;
+    for (; pulse < pulses; pulse += gridDim.x) {
+        const bool ok = mbar_wait_bounded(bar, phase);
+        if (__syncthreads_or(!ok)) {
+            if (t == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
+            timed_out = true;
+            break;
+        }
+        phase ^= 1u;
+        if (t == 0 && pulse + (int)gridDim.x < pulses) {
+            const char* from = reinterpret_cast<const char*>(src.row(pulse + gridDim.x));
+            for (uint32_t off = 0; off < bytes; off += kChunk)
+                bulk_prefetch_l2(from + off, bytes - off < kChunk ? bytes - off : kChunk);
+        }
+        float2 v[LP::E];
+#pragma unroll
+        for (int r = 0; r < LP::E; ++r) {
+            const int e = t + LP::T * r;
+            v[r] = e < copy ? sm[e] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        local_fft_forward<LP>(v, sm, t, twiddle, tab);
+        tmem_multiply<LP::E, false>(v, spec_cols);
+        local_fft_inverse<LP>(v, sm, t, twiddle_conj, tab);
+        fence_proxy_async_smem();
+        __syncthreads();
+        const int next = pulse + gridDim.x;
+        if (t == 0 && next < pulses) issue(next);
+        float2* yr = y + (size_t)pulse * N;
+#pragma unroll
+        for (int r = 0; r < LP::E; ++r) yr[t + LP::T * r] = v[r];  // stays in L2 for the next stage
+    }
+    // every warp is done with tensor memory (on the timeout path too): release it.  A
+    // timed-out CTA waits (bounded) for its copy still in flight before leaving.
+    if (timed_out && t == 0) (void)mbar_wait_bounded(bar, phase);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, kCols);
     }
 }
 
@@ -397,12 +542,63 @@ int replica_impl(const float2* h, int length, int normalize, int kind, const flo
     return ZKX_SUCCESS;
 }
 
+template <int N>
+constexpr size_t local_compression_smem()
+{
+    using LP = LocalPlan<N>;
+    return ((size_t)LP::EXCHANGE + 2 + LP::TABLE + (size_t)LP::T * (ilog2(LP::E) | 1)) * sizeof(float2);
+}
+
+// CTAs of the four-step compression kernel resident on the whole GPU at once.
+template <int N>
+int local_compression_slots(int* slots)
+{
+    using LP = LocalPlan<N>;
+    int dev = 0, sms = 0, per_sm = 0;
+    ZKX_CUDA(cudaGetDevice(&dev));
+    ZKX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    auto k = pulse_compression_local_kernel<N, RowsContiguous>;
+    const size_t smem = local_compression_smem<N>();
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ZKX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, LP::T, smem));
+    *slots = sms * std::max(per_sm, 1);
+    return ZKX_SUCCESS;
+}
+
+// The default kernel for the four-step lengths: the persistent kernel once every resident
+// CTA gets at least four pulses (its set-up per CTA and its pipelining then pay off), the
+// one-launch-per-pulse kernel below that (measured: 1024 x 16384 265.8 vs 278.5 us for the
+// chain; 256 x 16384 91.1 vs 83.8; 512 x 8192 90.3 vs 85.7; 1024 x 4096 91.9 vs 81.7).
+int default_variant_for(int pulses, int slots)
+{
+    return pulses >= 4 * slots ? ZKX_COMPRESSION_LOCAL : ZKX_COMPRESSION_PLAIN;
+}
+
 template <int N, class Src>
 int compression_impl(const Src& x, bool aligned16, int pulses, int samples, const float2* spectrum,
                      float2* y, int variant, cudaStream_t s)
 {
     if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
     using PL = FftPlan<N, elems_for(N)>;
+    if constexpr (local_fft_for(N)) {
+        if (variant == ZKX_COMPRESSION_DEFAULT) {
+            int slots = 0;
+            ZKX_TRY(local_compression_slots<N>(&slots));
+            variant = default_variant_for(pulses, slots);
+        }
+        if (aligned16 && variant == ZKX_COMPRESSION_LOCAL) {
+            using LP = LocalPlan<N>;
+            int slots = 0;
+            ZKX_TRY(local_compression_slots<N>(&slots));
+            const size_t smem = local_compression_smem<N>();
+            auto k = pulse_compression_local_kernel<N, Src>;
+            ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            const int grid = std::max(1, std::min(pulses, slots));
+            k<<<grid, LP::T, smem, s>>>(x, pulses, samples, spectrum, y, twiddle_table(), kernel_error_word());
+            ZKX_LAUNCHED("pulse_compression_local_kernel");
+            return ZKX_SUCCESS;
+        }
+    }
     if constexpr (N >= 4096) {
         // persistent bulk-copy pipeline: 16-byte aligned pulses (even length, aligned bases);
         // variant ZKX_COMPRESSION_PLAIN keeps the one-launch-per-pulse-group kernel
@@ -553,9 +749,23 @@ int launch_pulse_compression_variant(const float2* x, int pulses, int samples, i
 #undef ZKX_CALL
 }
 
+int resolve_compression_variant(int pulses, int nfft, int variant, int* resolved)
+{
+    *resolved = variant;
+    if (variant != ZKX_COMPRESSION_DEFAULT || !is_pow2(nfft) || !local_fft_for(nfft)) return ZKX_SUCCESS;
+    int slots = 0;
+    switch (nfft) {
+    case 4096: ZKX_TRY(local_compression_slots<4096>(&slots)); break;
+    case 8192: ZKX_TRY(local_compression_slots<8192>(&slots)); break;
+    default: ZKX_TRY(local_compression_slots<16384>(&slots)); break;
+    }
+    *resolved = default_variant_for(pulses, slots);
+    return ZKX_SUCCESS;
+}
+
 int launch_pulse_compression_table(const float2* const* cpis, int count, int pulses_per_cpi,
                                    int samples, int nfft, const float2* spectrum, float2* y,
-                                   cudaStream_t stream)
+                                   int variant, cudaStream_t stream)
 {
     if (count < 1 || count > kMaxRowTable)
         return fail(ZKX_INVALID_ARGUMENT, "pulse_compression: 1 to 64 CPIs per table launch");
@@ -571,7 +781,7 @@ int launch_pulse_compression_table(const float2* const* cpis, int count, int pul
     if (!is_pow2(nfft)) return launch_compression_any(src, pulses, samples, nfft, spectrum, y, stream);
     if (nfft > (1 << kMaxSmemFftLog))
         return launch_long_compression(src, pulses, samples, nfft, spectrum, y, stream);
-#define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, ZKX_COMPRESSION_DEFAULT, stream)
+#define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, variant, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
 #undef ZKX_CALL
 }

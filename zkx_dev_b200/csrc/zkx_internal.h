@@ -97,11 +97,17 @@ int launch_long_compression(const RowsContiguous& x, int pulses, int samples, in
                             const float2* spectrum, float2* y, cudaStream_t stream);
 int launch_long_compression(const RowsTable& x, int pulses, int samples, int nfft,
                             const float2* spectrum, float2* y, cudaStream_t stream);
+// The concrete ZKX_COMPRESSION_* kernel that `variant` stands for at `pulses` pulses of
+// nfft points (ZKX_COMPRESSION_DEFAULT resolves by the four-step kernels' rule; any other
+// value is returned as is).  Plans resolve it once from their per-CPI shape, so a CPI gives
+// the same bits alone and inside any batch.
+int resolve_compression_variant(int pulses, int nfft, int variant, int* resolved);
 // Range compression of `count` CPIs [pulses_per_cpi, samples] read in place from
 // separate buffers (count <= kMaxRowTable); y is [count * pulses_per_cpi, nfft].
+// `variant` is a ZKX_COMPRESSION_* choice, as for launch_pulse_compression_variant.
 int launch_pulse_compression_table(const float2* const* cpis, int count, int pulses_per_cpi,
                                    int samples, int nfft, const float2* spectrum, float2* y,
-                                   cudaStream_t stream);
+                                   int variant, cudaStream_t stream);
 int launch_long_fft_rows(const float2* x, int rows, int n, int inverse, float2* y,
                          cudaStream_t stream);
 int launch_doppler_window(int pulses, int window_kind, const float* explicit_window, float* out,
