@@ -46,6 +46,7 @@ enum {
     ZKX_CUDA_RUNTIME_ERROR = 2002,
     ZKX_OUT_OF_MEMORY = 2003,
     ZKX_BACKEND_ERROR = 2099,
+    ZKX_RESOURCE_FAILED = 3002,
     ZKX_INTERNAL_ERROR = 9001
 };
 
@@ -99,6 +100,12 @@ ZKX_API const char* zkx_version(void);
  * left without computing).  clear != 0 resets the word.  No counterpart in the
  * reference, whose kernels have no device-side waits. */
 ZKX_API int zkx_kernel_status(int clear, int* code);
+
+/* Self-test of that failure path (for tests and health checks; no counterpart in the
+ * reference): one 32-thread CTA waits on a barrier that no copy completes, gives up
+ * after limit_clocks SM clocks (1000 .. 2^31), records code 1 in the error word and
+ * returns.  Nothing is left running; read the result with zkx_kernel_status. */
+ZKX_API int zkx_selftest_wait_timeout(long long limit_clocks, zkx_stream_t stream);
 
 /* pulse_compression: y[p, :] = IFFT(FFT(x[p, :nfft]) * conj(FFT(w*h/||w*h||, nfft))).
  * Replaces cusignal::pulse_compression_device<float>
@@ -427,7 +434,9 @@ ZKX_API int zkx_rd_execute_batch(zkx_rd_plan plan, const void* x, int batch, voi
 enum {
     ZKX_COMPRESSION_DEFAULT = 0,
     ZKX_COMPRESSION_PLAIN = 1,       /* one launch per group of pulses */
-    ZKX_COMPRESSION_PERSISTENT = 2   /* persistent CTAs prefetching the next pulse (N >= 4096) */
+    ZKX_COMPRESSION_PERSISTENT = 2,  /* persistent CTAs prefetching the next pulse (N >= 4096) */
+    ZKX_COMPRESSION_LOCAL = 3        /* the persistent kernel with a four-step transform whose
+                                        later passes stay inside warps (N = 4096, 8192, 16384) */
 };
 typedef struct {
     int compression_variant;  /* ZKX_COMPRESSION_* */
@@ -483,6 +492,9 @@ typedef struct {
     int max_batch;           /* CPIs of one shape fused into one batch (16, at most 64) */
     double hbm_fraction;     /* budget = this fraction of the free HBM at creation (0.8) */
     size_t budget_bytes;     /* nonzero: a lower cap on the budget */
+    int max_pending;         /* submitted requests waiting for admission (0 = no bound); a
+                                submit beyond it is refused at once with ZKX_RESOURCE_FAILED,
+                                so an overloaded server sheds load instead of queueing it */
 } zkx_rd_server_desc;
 
 /* One CPI.  x and the outputs may be host memory (page-locked for the copies to
@@ -513,6 +525,7 @@ typedef struct {
     size_t peak_bytes;       /* most workspace-block bytes held at once (in flight + idle) */
     size_t plan_bytes;       /* resident replica spectra and Doppler windows */
     int plans;
+    uint64_t refused;        /* submits refused because max_pending requests were waiting */
 } zkx_rd_server_stats;
 
 typedef struct zkx_rd_server_s* zkx_rd_server;
@@ -522,7 +535,9 @@ ZKX_API int zkx_rd_server_create(const zkx_rd_server_desc* desc, zkx_rd_server* 
 /* Finishes every submitted request, then releases the loop. */
 ZKX_API int zkx_rd_server_destroy(zkx_rd_server server);
 /* Queues one CPI and returns at once with its ticket.  A request whose workspace
- * alone exceeds the budget is refused with ZKX_OUT_OF_MEMORY. */
+ * alone exceeds the budget is refused with ZKX_OUT_OF_MEMORY; with max_pending set, a
+ * request arriving while that many wait for admission is refused with
+ * ZKX_RESOURCE_FAILED (no ticket; the caller may retry or drop it). */
 ZKX_API int zkx_rd_submit(zkx_rd_server server, const zkx_rd_request* request, uint64_t* ticket);
 /* *done = 1 and the request's status once it has completed (the ticket is then
  * released); *done = 0 if it is still pending after timeout_ms (0 = do not wait,

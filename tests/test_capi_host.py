@@ -134,3 +134,10 @@ def test_reference_doppler_phase_error_grows_with_pulses():
         errs.append(np.linalg.norm(a - b) / np.linalg.norm(b))
     assert 3e-6 < errs[0] < 1.5e-5
     assert errs[2] > 8 * errs[0]
+
+
+def test_wait_timeout_selftest_checks_its_limit(L):
+    """The failure-path self-test refuses limits outside 1000 .. 2^31 clocks before any
+    device work (so this runs without a GPU)."""
+    for bad in (0, 999, (1 << 31) + 1):
+        assert L.lib().zkx_selftest_wait_timeout(bad, None) == L.INVALID_ARGUMENT

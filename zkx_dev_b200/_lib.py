@@ -17,6 +17,7 @@ INVALID_ARGUMENT = 1001
 INVALID_SHAPE = 1002
 UNSUPPORTED_OPERATION = 1004
 OUT_OF_MEMORY = 2003
+RESOURCE_FAILED = 3002
 
 WINDOW_NONE, WINDOW_HANN, WINDOW_HAMMING, WINDOW_EXPLICIT_FP32, WINDOW_EXPLICIT_FP64 = range(5)
 CFAR_ACCURATE, CFAR_COMPAT = 0, 1
@@ -52,7 +53,7 @@ class ServerDesc(ctypes.Structure):
     _fields_ = [("normalize", _I), ("range_window", _I), ("doppler_window", _I),
                 ("guard_cells", _I * 2), ("reference_cells", _I * 2), ("pfa", _D),
                 ("cfar_mode", _I), ("streams", _I), ("max_inflight", _I), ("max_batch", _I),
-                ("hbm_fraction", _D), ("budget_bytes", ctypes.c_size_t)]
+                ("hbm_fraction", _D), ("budget_bytes", ctypes.c_size_t), ("max_pending", _I)]
 
 
 class Request(ctypes.Structure):
@@ -66,7 +67,8 @@ class ServerStats(ctypes.Structure):
                 ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("mean_batch", _D),
                 ("p50_us", _D), ("p99_us", _D), ("max_us", _D), ("mean_us", _D),
                 ("cpis_per_s", _D), ("budget_bytes", ctypes.c_size_t),
-                ("peak_bytes", ctypes.c_size_t), ("plan_bytes", ctypes.c_size_t), ("plans", _I)]
+                ("peak_bytes", ctypes.c_size_t), ("plan_bytes", ctypes.c_size_t), ("plans", _I),
+                ("refused", ctypes.c_uint64)]
 
 
 class SynthTarget(ctypes.Structure):
@@ -77,6 +79,7 @@ SIGNATURES = {
     "zkx_last_error": (ctypes.c_char_p, []),
     "zkx_version": (ctypes.c_char_p, []),
     "zkx_kernel_status": (_I, [_I, ctypes.POINTER(_I)]),
+    "zkx_selftest_wait_timeout": (_I, [ctypes.c_longlong, _P]),
     "zkx_pulse_compression_c64": (_I, [_P, _I, _I, _P, _I, _I, _I, _I, _P, _P, _P]),
     "zkx_pulse_compression_c64_noalloc": (_I, [_P, _I, _I, _P, _I, _I, _I, _I, _P, _P, _P]),
     "zkx_replica_spectrum_c64": (_I, [_P, _I, _I, _I, _I, _P, _P, _P]),

@@ -174,6 +174,43 @@ int stream_workspace(std::size_t bytes, cudaStream_t stream, void** out)
 
 }  // namespace zkx
 
+namespace zkx {
+namespace {
+
+// The failure path of every bulk-copy wait, exercised on purpose: thread 0 arms the
+// barrier for 16 bytes that no copy will deliver (none is issued, so nothing is in flight
+// when the CTA leaves), every thread waits with the bounded wait the kernels use, the CTA
+// agrees on the timeout and records it in the error word exactly as they do.
+__global__ void wait_timeout_selftest_kernel(long long limit, int* err)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_arrive_expect_tx(&bar, 16);
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0, limit);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
+        return;
+    }
+}
+
+}  // namespace
+}  // namespace zkx
+
+extern "C" int zkx_selftest_wait_timeout(long long limit_clocks, zkx_stream_t stream)
+{
+    using namespace zkx;
+    if (limit_clocks < 1000 || limit_clocks > (1LL << 31))
+        return fail(ZKX_INVALID_ARGUMENT, "selftest_wait_timeout: limit must be 1000 .. 2^31 clocks");
+    ZKX_TRY(ensure_device_ready());
+    wait_timeout_selftest_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(limit_clocks,
+                                                                                 kernel_error_word());
+    ZKX_LAUNCHED("wait_timeout_selftest_kernel");
+    return ZKX_SUCCESS;
+}
+
 extern "C" const char* zkx_last_error(void) { return zkx::g_error.c_str(); }
 
 extern "C" int zkx_kernel_status(int clear, int* code)

@@ -44,12 +44,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase)
     return done != 0;
 }
 
-// Bounded wait: true when the phase completed, false after ~2^31 SM clocks.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase)
+// Bounded wait: true when the phase completed, false after `limit` SM clocks (by default
+// 2^31, about one second).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, long long limit = 1LL << 31)
 {
     const long long start = clock64();
     while (!mbar_try_wait(bar, phase)) {
-        if (clock64() - start > (1LL << 31)) return false;
+        if (clock64() - start > limit) return false;
     }
     return true;
 }
