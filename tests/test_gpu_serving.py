@@ -181,6 +181,34 @@ def test_admission_tight_budget_counts_every_block(z):
         assert torch.equal(det, alone(z, c, P, N)["detections"])
 
 
+def test_max_pending_sheds_load(z):
+    """With max_pending = 4, submits that arrive while four requests wait for admission
+    are refused at once with 3002 (no ticket), counted in the statistics, and every
+    accepted request still completes with the result it gets alone."""
+    from zkx_dev_b200.synth import make_cpi
+    P, N = 256, 8192
+    cpi = make_cpi(P, N, 8, 512, seed=811)
+    x = torch.as_tensor(cpi.x).cuda()
+    rep = torch.as_tensor(cpi.replica).cuda()
+    accepted, refused = [], 0
+    with z.RdServer(z.ServerConfig(max_pending=4, max_batch=1, streams=1, max_inflight=1)) as server:
+        for _ in range(64):
+            det = torch.empty((P, N), dtype=torch.uint8, device="cuda")
+            try:
+                accepted.append((server.submit(x, rep, 5, det), det))
+            except z.ZkxError as e:
+                assert e.code == 3002
+                refused += 1
+        for t, _ in accepted:
+            server.wait(t)
+        st = server.stats()
+    assert refused > 0 and st["refused"] == refused
+    assert st["completed"] == len(accepted)
+    ref = alone(z, cpi, P, N)["detections"]
+    for _, det in accepted:
+        assert torch.equal(det.cpu(), ref)
+
+
 def test_oversized_request_is_refused(z):
     with z.RdServer(z.ServerConfig(budget_bytes=1 << 20)) as server:
         x = torch.zeros((64, 4096), dtype=torch.complex64)

@@ -21,9 +21,9 @@
 // more requests without waiting for the rest of the device work: requests that arrive
 // while others are on the GPU join as soon as slots and memory free up.
 //
-// Workspaces are device blocks the server keeps: a batch takes an idle block of its size
-// (up to 1.5x) or a new one, and gives it back from its completion callback, when every
-// copy and kernel that used it has finished.  After the first batches of each shape no
+// Workspaces are device blocks the server keeps: a batch takes the smallest idle block that
+// is large enough, or a new one within the budget, and gives it back from its completion
+// callback, when every copy and kernel that used it has finished.  After the first batches of each shape no
 // allocation happens at all, and no stream ever waits for another batch's memory.
 //
 // Plans (replica spectrum and Doppler window, resident) are cached per (pulses,
@@ -136,7 +136,7 @@ struct zkx_rd_server_s {
     unsigned next_stream = 0;
 
     std::vector<double> latency_us;
-    uint64_t submitted = 0, completed = 0, failed = 0, batches = 0, batched_cpis = 0;
+    uint64_t submitted = 0, completed = 0, failed = 0, batches = 0, batched_cpis = 0, refused = 0;
     Clock::time_point first_submit, last_done;
     bool have_first = false;
 };
@@ -534,6 +534,7 @@ extern "C" int zkx_rd_server_create(const zkx_rd_server_desc* desc, zkx_rd_serve
     if (d.max_inflight <= 0) d.max_inflight = 2 * d.streams;
     if (d.max_batch <= 0) d.max_batch = 16;
     if (d.hbm_fraction <= 0) d.hbm_fraction = 0.8;
+    if (d.max_pending < 0) return fail(ZKX_INVALID_ARGUMENT, "rd_server_create: max_pending must be >= 0");
     if (d.hbm_fraction > 1 || d.streams > 64 || d.max_batch > kMaxRowTable)
         return fail(ZKX_INVALID_ARGUMENT,
                     "rd_server_create: hbm_fraction <= 1, streams <= 64 and max_batch <= 64 required");
@@ -622,6 +623,11 @@ extern "C" int zkx_rd_submit(zkx_rd_server s, const zkx_rd_request* r, uint64_t*
             delete q;
             return fail(ZKX_INVALID_ARGUMENT, "rd_submit: server is shutting down");
         }
+        if (s->d.max_pending > 0 && s->pending.size() >= (size_t)s->d.max_pending) {
+            delete q;
+            ++s->refused;
+            return fail(ZKX_RESOURCE_FAILED, "rd_submit: max_pending requests are waiting for admission");
+        }
         q->ticket = s->next_ticket++;
         q->submitted = Clock::now();
         if (!s->have_first) {
@@ -693,6 +699,7 @@ extern "C" int zkx_rd_server_stats_get(zkx_rd_server s, zkx_rd_server_stats* out
     st.peak_bytes = s->peak;
     st.plan_bytes = s->plan_bytes;
     st.plans = (int)s->plans.size();
+    st.refused = s->refused;
     *out = st;
     return ZKX_SUCCESS;
 }
@@ -702,7 +709,7 @@ extern "C" int zkx_rd_server_stats_reset(zkx_rd_server s)
     if (!s) return fail(ZKX_INVALID_ARGUMENT, "rd_server_stats: null pointer");
     std::lock_guard<std::mutex> lk(s->mu);
     s->latency_us.clear();
-    s->submitted = s->completed = s->failed = s->batches = s->batched_cpis = 0;
+    s->submitted = s->completed = s->failed = s->batches = s->batched_cpis = s->refused = 0;
     s->have_first = false;
     s->peak = s->held;
     return ZKX_SUCCESS;

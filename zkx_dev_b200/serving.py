@@ -30,6 +30,7 @@ class ServerConfig:
     max_batch: int = 16
     hbm_fraction: float = 0.8
     budget_bytes: int = 0      # 0: no cap below hbm_fraction of free HBM
+    max_pending: int = 0       # 0: unbounded queue; else submits beyond it raise ZkxError 3002
 
 
 def _check_buffer(t: Optional[torch.Tensor], shape, dtype, name: str, required: bool = False):
@@ -59,6 +60,7 @@ class RdServer:
         d.max_batch = cfg.max_batch
         d.hbm_fraction = cfg.hbm_fraction
         d.budget_bytes = cfg.budget_bytes
+        d.max_pending = cfg.max_pending
         h = ctypes.c_void_p()
         L.check(L.lib().zkx_rd_server_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h
