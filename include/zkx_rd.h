@@ -438,9 +438,15 @@ enum {
     ZKX_COMPRESSION_LOCAL = 3        /* the persistent kernel with a four-step transform whose
                                         later passes stay inside warps (N = 4096, 8192, 16384) */
 };
+enum {
+    ZKX_CFAR_TILE_DEFAULT = 0,
+    ZKX_CFAR_TILE_FULL = 1,    /* 64 x 64 tile, row-sum planes of the whole tile (3 CTAs per SM) */
+    ZKX_CFAR_TILE_HALVES = 2   /* 64 x 64 tile, row-sum planes built in two 32-row halves (4 CTAs per SM) */
+};
 typedef struct {
     int compression_variant;  /* ZKX_COMPRESSION_* */
     int doppler_columns;      /* range columns per CTA of the bulk-copy Doppler kernel: 8 or 16 */
+    int cfar_tile;            /* ZKX_CFAR_TILE_* (accurate-mode CA-CFAR of the tiled window sizes) */
 } zkx_rd_tuning;
 
 /* Times every candidate of each stage on `batch` CPIs at x (device, the plan's shape) on

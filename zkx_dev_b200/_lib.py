@@ -46,7 +46,7 @@ class RdDesc(ctypes.Structure):
 
 
 class RdTuning(ctypes.Structure):
-    _fields_ = [("compression_variant", _I), ("doppler_columns", _I)]
+    _fields_ = [("compression_variant", _I), ("doppler_columns", _I), ("cfar_tile", _I)]
 
 
 class ServerDesc(ctypes.Structure):

@@ -132,13 +132,15 @@ class RangeDopplerChain:
         t = L.RdTuning()
         L.check(L.lib().zkx_rd_plan_autotune(self._plan, x.data_ptr(), batch, L.stream_handle(),
                                              ctypes.byref(t)))
-        return {"compression_variant": t.compression_variant, "doppler_columns": t.doppler_columns}
+        return {"compression_variant": t.compression_variant, "doppler_columns": t.doppler_columns,
+                "cfar_tile": t.cfar_tile}
 
     @property
     def tuning(self) -> Dict[str, int]:
         t = L.RdTuning()
         L.check(L.lib().zkx_rd_plan_get_tuning(self._plan, ctypes.byref(t)))
-        return {"compression_variant": t.compression_variant, "doppler_columns": t.doppler_columns}
+        return {"compression_variant": t.compression_variant, "doppler_columns": t.doppler_columns,
+                "cfar_tile": t.cfar_tile}
 
     def close(self) -> None:
         if getattr(self, "_plan", None) is not None and self._plan.value:

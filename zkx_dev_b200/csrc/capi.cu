@@ -218,7 +218,7 @@ extern "C" int zkx_ca_cfar_f32(const float* x, int rank, int rows, int cols, int
                                      detections, stream);
     }
     return launch_ca_cfar_accurate(x, rows, cols, gr, gc, rr, rc, g.alpha, g.nref, threshold,
-                                   detections, 1, stream);
+                                   detections, 1, ZKX_CFAR_TILE_DEFAULT, stream);
 }
 
 // --------------------------------------------------------------------- filters
@@ -574,7 +574,7 @@ int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compresse
         return ZKX_SUCCESS;
     }
     return launch_ca_cfar_accurate(power, nd, nr, gd[0], gd[1], rf[0], rf[1], p->cfar.alpha,
-                                   p->cfar.nref, threshold, detections, batch, stream);
+                                   p->cfar.nref, threshold, detections, batch, p->tuning.cfar_tile, stream);
 }
 }  // namespace zkx
 
@@ -674,6 +674,34 @@ extern "C" int zkx_rd_plan_autotune(zkx_rd_plan p, const void* x, int batch, zkx
             }
         }
     }
+    if (rc == ZKX_SUCCESS && p->d.cfar_mode == ZKX_CFAR_ACCURATE) {
+        // both CA-CFAR kernels on the power map the Doppler candidates left behind
+        float* thr = nullptr;
+        uint8_t* det = nullptr;
+        cudaError_t ea = cudaMalloc(&thr, map * sizeof(float));
+        if (ea == cudaSuccess) ea = cudaMalloc(&det, map);
+        if (ea != cudaSuccess) {
+            rc = cuda_status(ea, "rd_plan_autotune allocation");
+        } else {
+            const int* gd = p->d.guard_cells;
+            const int* rf = p->d.reference_cells;
+            float tbest = 0.f;
+            for (int tile : {ZKX_CFAR_TILE_FULL, ZKX_CFAR_TILE_HALVES}) {
+                float ms = 0.f;
+                rc = time_median([&] {
+                    return launch_ca_cfar_accurate(power, nd, nr, gd[0], gd[1], rf[0], rf[1], p->cfar.alpha,
+                                                   p->cfar.nref, thr, det, batch, tile, stream);
+                }, stream, &ms);
+                if (rc != ZKX_SUCCESS) break;
+                if (tile == ZKX_CFAR_TILE_FULL || ms < tbest) {
+                    tbest = ms;
+                    best.cfar_tile = tile;
+                }
+            }
+        }
+        cudaFree(thr);
+        cudaFree(det);
+    }
     cudaFree(comp);
     cudaFree(power);
     if (rc != ZKX_SUCCESS) return rc;
@@ -697,7 +725,8 @@ extern "C" int zkx_rd_plan_set_tuning(zkx_rd_plan p, const zkx_rd_tuning* t)
 {
     if (!p || !t) return fail(ZKX_INVALID_ARGUMENT, "rd_plan_set_tuning: null pointer");
     if (t->compression_variant < 0 || t->compression_variant > ZKX_COMPRESSION_LOCAL ||
-        (t->doppler_columns != 0 && t->doppler_columns != 8 && t->doppler_columns != 16))
+        (t->doppler_columns != 0 && t->doppler_columns != 8 && t->doppler_columns != 16) ||
+        t->cfar_tile < 0 || t->cfar_tile > ZKX_CFAR_TILE_HALVES)
         return fail(ZKX_INVALID_ARGUMENT, "rd_plan_set_tuning: unknown kernel choice");
     p->tuning = *t;
     return ZKX_SUCCESS;

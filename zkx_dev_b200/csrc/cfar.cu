@@ -377,6 +377,151 @@ cfar_accurate_tma_kernel(const __grid_constant__ CUtensorMap tmap, int rows, int
     }
 }
 
+// Second TMA variant: the same tile, halo copy, separable sums and FP64 re-check, with the
+// row-sum planes built and consumed in two 32-row halves, so they take half the shared
+// memory (about 55 KB per CTA: four CTAs per SM instead of three, at most 64 registers per
+// thread), and the horizontal pass reads them with 128-bit loads (plane pitch = 4 modulo
+// 32 words: eight consecutive rows of a quarter-warp land on distinct bank groups).
+// A thread of the horizontal pass owns 8 cells of one row; a vertical item is 16 rows of
+// one halo column.
+template <int GR, int GC, int RR, int RC>
+struct CfarTma2Geom {
+    using G = CfarTmaGeom<GR, GC, RR, RC>;
+    static constexpr int HALF = kCfarTY / 2;
+    static constexpr int PITCH = ((G::HC + 27) / 32) * 32 + 4;   // >= HC, = 4 (mod 32)
+    static constexpr size_t smem_bytes()
+    {
+        return (size_t)G::HR * G::BOXW * sizeof(float) + (size_t)2 * HALF * PITCH * sizeof(float) + 16;
+    }
+    static_assert(PITCH >= G::HC && PITCH % 32 == 4, "plane pitch");
+};
+
+template <int GR, int GC, int RR, int RC>
+__global__ void __launch_bounds__(kCfarThreads, 4)
+cfar_accurate_tma2_kernel(const __grid_constant__ CUtensorMap tmap, int rows, int cols,
+                          float scale32, double scale64, float* __restrict__ thr,
+                          uint8_t* __restrict__ det, int* err)
+{
+    using G = CfarTmaGeom<GR, GC, RR, RC>;
+    using G2 = CfarTma2Geom<GR, GC, RR, RC>;
+    constexpr int MR = G::MR, MC = G::MC, HC = G::HC, OFF = G::OFF, BOXW = G::BOXW;
+    constexpr int PITCH = G2::PITCH, HALF = G2::HALF, TY = kCfarTY, TX = kCfarTX;
+    static_assert(((MC + OFF) & 3) == 0 && (BOXW & 3) == 0, "128-bit cell loads");
+    extern __shared__ __align__(128) float csm[];
+    float* P = csm;                        // [HR][BOXW]; halo column hc at P[.. + hc + OFF]
+    float* SA = P + G::HR * BOXW;          // [HALF][PITCH]
+    float* SB = SA + HALF * PITCH;         // [HALF][PITCH]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(SB + HALF * PITCH);
+    const int r0 = blockIdx.y * TY;
+    const int c0 = blockIdx.x * TX;
+    const int map_row0 = blockIdx.z * rows;
+    thr += (size_t)blockIdx.z * rows * cols;
+    det += (size_t)blockIdx.z * rows * cols;
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(bar, (uint32_t)(G::HR * BOXW * sizeof(float)));
+        tma_load_2d(P, &tmap, c0 - MC - OFF, map_row0 + r0 - MR, bar);
+    }
+    const bool ok = mbar_wait_bounded(bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
+        return;
+    }
+    constexpr int SEG = 16, VL = SEG + 2 * MR;
+    constexpr int CS = 8, HL = CS + 2 * MC, HL4 = (HL + 3) / 4;
+    const int hr = threadIdx.x & 31;          // horizontal: row within the half
+    const int cb = (threadIdx.x >> 5) * CS;    // horizontal: first of 8 columns
+    for (int h = 0; h < 2; ++h) {
+        // vertical pieces of rows [h HALF, h HALF + HALF): one item per (halo column, 16 rows)
+        for (int item = threadIdx.x; item < HC * (HALF / SEG); item += kCfarThreads) {
+            const int seg = item / HC;
+            const int hc = item - seg * HC;
+            const int rb = h * HALF + seg * SEG;
+            float v[VL];
+#pragma unroll
+            for (int i = 0; i < VL; ++i) v[i] = P[(rb + i) * BOXW + hc + OFF];
+            float wt[VL - RR + 1], wg[VL - 2 * GR];
+            window_sums<RR, VL>(v, wt);
+            window_sums<2 * GR + 1, VL>(v, wg);
+#pragma unroll
+            for (int r = 0; r < SEG; ++r) {
+                SA[(seg * SEG + r) * PITCH + hc] = wt[r] + wt[r + MR + GR + 1];
+                SB[(seg * SEG + r) * PITCH + hc] = wg[r + MR - GR];
+            }
+        }
+        __syncthreads();
+        const int tr = h * HALF + hr;          // row within the tile
+        const int grow = r0 + tr;
+        if (grow < rows) {
+            float a[HL4 * 4], b[HL4 * 4];
+#pragma unroll
+            for (int q = 0; q < HL4; ++q) {
+                const float4 fa = *reinterpret_cast<const float4*>(SA + hr * PITCH + cb + 4 * q);
+                const float4 fb = *reinterpret_cast<const float4*>(SB + hr * PITCH + cb + 4 * q);
+                a[4 * q] = fa.x; a[4 * q + 1] = fa.y; a[4 * q + 2] = fa.z; a[4 * q + 3] = fa.w;
+                b[4 * q] = fb.x; b[4 * q + 1] = fb.y; b[4 * q + 2] = fb.z; b[4 * q + 3] = fb.w;
+            }
+            float wa[HL - 2 * MC], wb[HL - RC + 1];
+            window_sums<2 * MC + 1, HL>(a, wa);
+            window_sums<RC, HL>(b, wb);
+            float xv[CS];
+            const float* prow = P + (tr + MR) * BOXW + cb + MC + OFF;
+#pragma unroll
+            for (int q = 0; q < CS / 4; ++q) {
+                const float4 f = reinterpret_cast<const float4*>(prow)[q];
+                xv[4 * q] = f.x; xv[4 * q + 1] = f.y; xv[4 * q + 2] = f.z; xv[4 * q + 3] = f.w;
+            }
+            const bool row_interior = grow >= MR && grow < rows - MR;
+            float tout[CS];
+            unsigned dlo = 0, dhi = 0;
+#pragma unroll
+            for (int j = 0; j < CS; ++j) {
+                const int gcol = c0 + cb + j;
+                float t = 0.f;
+                bool hit;
+                if (row_interior && gcol >= MC && gcol < cols - MC) {
+                    const float ring = wa[j] + (wb[j] + wb[j + MC + GC + 1]);
+                    t = scale32 * ring;
+                    hit = xv[j] > t;
+                    if (fabsf(xv[j] - t) <= kRecheckBand * t) {
+                        double s = 0.0;
+                        for (int dr = -MR; dr <= MR; ++dr)
+                            for (int dc = -MC; dc <= MC; ++dc)
+                                if (dr < -GR || dr > GR || dc < -GC || dc > GC)
+                                    s += (double)P[(tr + MR + dr) * BOXW + cb + j + MC + OFF + dc];
+                        const double t64 = scale64 * s;
+                        hit = (double)xv[j] > t64;
+                        t = (float)t64;
+                    }
+                } else {
+                    hit = xv[j] > 0.f;
+                }
+                tout[j] = t;
+                if (j < 4) dlo |= (hit ? 1u : 0u) << (8 * j);
+                else dhi |= (hit ? 1u : 0u) << (8 * (j - 4));
+            }
+            const int cstart = c0 + cb;
+            float* trow = thr + (size_t)grow * cols + cstart;
+            uint8_t* drow = det + (size_t)grow * cols + cstart;
+            if (cstart + CS <= cols && ((reinterpret_cast<uintptr_t>(trow) & 15) == 0) &&
+                ((reinterpret_cast<uintptr_t>(drow) & 7) == 0)) {
+                reinterpret_cast<float4*>(trow)[0] = make_float4(tout[0], tout[1], tout[2], tout[3]);
+                reinterpret_cast<float4*>(trow)[1] = make_float4(tout[4], tout[5], tout[6], tout[7]);
+                *reinterpret_cast<uint2*>(drow) = make_uint2(dlo, dhi);
+            } else {
+#pragma unroll
+                for (int j = 0; j < CS; ++j)
+                    if (cstart + j < cols) {
+                        trow[j] = tout[j];
+                        drow[j] = (uint8_t)(((j < 4 ? dlo : dhi) >> (8 * (j & 3))) & 1u);
+                    }
+            }
+        }
+        __syncthreads();  // the next half's vertical pass overwrites SA and SB
+    }
+}
+
 // Any window geometry: one thread per cell, ring summed directly in FP64.
 __global__ void cfar_generic_kernel(const float* __restrict__ x, int rows, int cols, int gr, int gc,
                                     int rr, int rc, double scale64, float* __restrict__ thr,
@@ -502,7 +647,7 @@ __global__ void compat_threshold_kernel(const float* __restrict__ x, const float
 
 template <int GR, int GC, int RR, int RC>
 int accurate_impl(const float* x, int rows, int cols, float s32, double s64, float* thr,
-                  uint8_t* det, int batch, cudaStream_t s)
+                  uint8_t* det, int batch, int tile, cudaStream_t s)
 {
     dim3 grid((cols + kCfarTX - 1) / kCfarTX, (rows + kCfarTY - 1) / kCfarTY, batch);
     using G = CfarTmaGeom<GR, GC, RR, RC>;
@@ -510,6 +655,15 @@ int accurate_impl(const float* x, int rows, int cols, float s32, double s64, flo
         CUtensorMap map;
         if (encode_tensor_map_2d_f32(&map, x, (uint64_t)cols, (uint64_t)rows * batch,
                                      (uint64_t)cols * sizeof(float), G::BOXW, G::HR)) {
+            if (tile == ZKX_CFAR_TILE_HALVES) {
+                using G2 = CfarTma2Geom<GR, GC, RR, RC>;
+                const size_t smem = G2::smem_bytes();
+                auto k = cfar_accurate_tma2_kernel<GR, GC, RR, RC>;
+                ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                k<<<grid, kCfarThreads, smem, s>>>(map, rows, cols, s32, s64, thr, det, kernel_error_word());
+                ZKX_LAUNCHED("cfar_accurate_tma2_kernel");
+                return ZKX_SUCCESS;
+            }
             const size_t smem = G::smem_bytes();
             auto k = cfar_accurate_tma_kernel<GR, GC, RR, RC>;
             ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -532,13 +686,13 @@ int accurate_impl(const float* x, int rows, int cols, float s32, double s64, flo
 
 int launch_ca_cfar_accurate(const float* x, int rows, int columns, int gr, int gc, int rr, int rc,
                             double alpha, int nref, float* threshold, uint8_t* detections,
-                            int batch, cudaStream_t stream)
+                            int batch, int tile, cudaStream_t stream)
 {
     if (batch < 1 || batch > 65535) return fail(ZKX_UNSUPPORTED_OPERATION, "ca_cfar: batch must be 1..65535");
     const double s64 = alpha / (double)nref;
     const float s32 = (float)s64;
 #define ZKX_CFAR_CASE(A, B, C, D) \
-    if (gr == A && gc == B && rr == C && rc == D) return accurate_impl<A, B, C, D>(x, rows, columns, s32, s64, threshold, detections, batch, stream);
+    if (gr == A && gc == B && rr == C && rc == D) return accurate_impl<A, B, C, D>(x, rows, columns, s32, s64, threshold, detections, batch, tile, stream);
     ZKX_CFAR_CASE(2, 2, 8, 8)
     ZKX_CFAR_CASE(1, 1, 4, 4)
     ZKX_CFAR_CASE(2, 2, 4, 4)

@@ -112,10 +112,12 @@ int launch_long_fft_rows(const float2* x, int rows, int n, int inverse, float2* 
                          cudaStream_t stream);
 int launch_doppler_window(int pulses, int window_kind, const float* explicit_window, float* out,
                           cudaStream_t stream);
+// `tile` is a ZKX_CFAR_TILE_* kernel choice for the tiled window sizes; every choice gives
+// the same detection mask (each re-decides near-threshold cells in FP64).
 int launch_ca_cfar_accurate(const float* x, int rows, int columns, int guard_rows,
                             int guard_columns, int reference_rows, int reference_columns,
                             double alpha, int reference_count, float* threshold,
-                            uint8_t* detections, int batch, cudaStream_t stream);
+                            uint8_t* detections, int batch, int tile, cudaStream_t stream);
 int launch_ca_cfar_compat(const float* x, int rank, int rows, int columns, int guard_rows,
                           int guard_columns, int reference_rows, int reference_columns,
                           float alpha, int reference_count, float* cumulative, float* threshold,
