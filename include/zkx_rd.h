@@ -434,9 +434,11 @@ ZKX_API int zkx_rd_execute_batch(zkx_rd_plan plan, const void* x, int batch, voi
 enum {
     ZKX_COMPRESSION_DEFAULT = 0,
     ZKX_COMPRESSION_PLAIN = 1,       /* one launch per group of pulses */
-    ZKX_COMPRESSION_PERSISTENT = 2,  /* persistent CTAs prefetching the next pulse (N >= 4096) */
-    ZKX_COMPRESSION_LOCAL = 3        /* the persistent kernel with a four-step transform whose
-                                        later passes stay inside warps (N = 4096, 8192, 16384) */
+    ZKX_COMPRESSION_PERSISTENT = 2,  /* persistent CTAs prefetching the next pulse (N 4096 .. 16384);
+                                        one cluster per pulse (N 32768, 65536) */
+    ZKX_COMPRESSION_LOCAL = 3        /* persistent CTAs (clusters above 16384 points) with a four-step
+                                        transform whose later passes stay inside warps and the
+                                        spectrum in tensor memory (N 4096 .. 65536) */
 };
 enum {
     ZKX_CFAR_TILE_DEFAULT = 0,

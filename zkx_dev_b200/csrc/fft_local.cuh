@@ -27,6 +27,7 @@
 #pragma once
 
 #include "fft_core.cuh"
+#include "tcgen05.cuh"
 
 namespace zkx {
 
@@ -153,6 +154,43 @@ __device__ __forceinline__ int local_bin(int t, int q)
     const int g = t / LP::P, u = t - g * LP::P;
     const int j = q / LP::P, k3 = q - j * LP::P;
     return g + LP::E * (u + LP::P * j) + LP::E * LP::E * k3;
+}
+
+// The spectrum bins a thread's registers hold after local_fft_forward, in register order,
+// into its own tensor-memory lane at `cols` (2E consecutive FP32 columns), read once from
+// the natural-order spectrum; then tmem_multiply applies them per transform.
+template <class LP>
+__device__ __forceinline__ void spectrum_to_tmem(const float2* __restrict__ spectrum, int t, uint32_t cols)
+{
+#pragma unroll
+    for (int c = 0; c < 2 * LP::E; c += 16) {
+        float sv[16];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float2 b = __ldg(&spectrum[local_bin<LP>(t, c / 2 + i)]);
+            sv[2 * i] = b.x;
+            sv[2 * i + 1] = b.y;
+        }
+        tmem_store16(cols + c, sv);
+    }
+    tmem_wait_store();
+}
+
+// v[k] *= s_k (CONJ: conj(s_k)) with s_k the complex word pair at columns 2k, 2k+1.
+template <int E, bool CONJ>
+__device__ __forceinline__ void tmem_multiply(float2 (&v)[E], uint32_t cols)
+{
+#pragma unroll
+    for (int c = 0; c < 2 * E; c += 16) {
+        float w[16];
+        tmem_load16(cols + c, w);
+        tmem_wait_load();
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float2 m = make_float2(w[2 * i], w[2 * i + 1]);
+            v[c / 2 + i] = CONJ ? cmulc(v[c / 2 + i], m) : cmul(v[c / 2 + i], m);
+        }
+    }
 }
 
 }  // namespace zkx

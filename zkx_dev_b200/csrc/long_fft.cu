@@ -18,9 +18,12 @@
 // not stall the sender), so each value crosses the SM-to-SM network at most once per
 // pass and the input and output cross HBM exactly once.  Range compression keeps the
 // spectrum in "cluster order" (bin k1 + R k2 at k1 M + k2) and never reorders.
+#include <algorithm>
+
 #include <cooperative_groups.h>
 
 #include "fft_core.cuh"
+#include "fft_local.cuh"
 #include "tma.cuh"
 #include "window.cuh"
 #include "zkx_internal.h"
@@ -253,6 +256,83 @@ long_compression_kernel(const Src src, int pulses, int samples,
     cross_dit_gather<R, 1>(cl, v, sm, k1, t, tw, y + pulse * (size_t)N, 1.0f);
 }
 
+// Persistent form of the kernel above: each cluster walks pulses cluster, +clusters, ...
+// (clusters = the clusters resident on the GPU), so the per-CTA set-up happens once: the
+// local sub-transform uses the four-step ordering of fft_local.cuh (one block-wide exchange
+// per direction), and the CTA's slice of the cluster-order spectrum sits in tensor memory
+// in the digit-reversed order that ordering leaves in registers (tcgen05.st once,
+// tcgen05.ld per pulse: 256 columns, one CTA per SM).  At the start of each pulse every
+// CTA pulls its slice of the cluster's next pulse into L2, so that pulse's cross-CTA pass
+// reads L2.  The cross-CTA passes are the same as above; their cluster barriers also order
+// one pulse's last reads of shared memory before the next pulse's remote writes.
+template <int R, class Src>
+__global__ void __cluster_dims__(R, 1, 1) __launch_bounds__(kT, 1)
+long_compression_local_kernel(const Src src, int pulses, int samples, const float2* __restrict__ spectrum,
+                              float2* __restrict__ y, const float2* __restrict__ tw)
+{
+    using LP = LocalPlan<kM>;
+    static_assert(LP::T == kT && LP::E == kE, "the local plan of the 16384-point sub-transform");
+    constexpr int LOGE = ilog2(kE);
+    constexpr uint32_t kCols = (kT / 128) * 2 * kE;
+    constexpr int N = R * kM;
+    constexpr int S = kM / R;
+    extern __shared__ __align__(128) float2 sm[];
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + LP::EXCHANGE);
+    float2* tab = sm + LP::EXCHANGE + 2;
+    const cg::cluster_group cl = cg::this_cluster();
+    const int k1 = (int)cl.block_rank();
+    const int t = threadIdx.x;
+    const int warp = t >> 5;
+    const int cluster = (int)(blockIdx.x / R), clusters = (int)(gridDim.x / R);
+    const int avail = samples < N ? samples : N;
+    if (warp == 0) {
+        tmem_alloc(tmem_slot, kCols);
+        tmem_relinquish();
+    }
+    float2* first = tab + LP::TABLE + t * (LOGE | 1);
+    fill_local_table<LP>(tab, t, kT, tw);
+    {
+        float2 wb[LOGE];
+        load_twiddle_bases<kE, LP::LOGN>(wb, t, tw);
+#pragma unroll
+        for (int b = 0; b < LOGE; ++b) first[b] = wb[b];
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const uint32_t spec_cols = tmem_base + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(warp >> 2) * (2 * kE);
+    spectrum_to_tmem<LP>(spectrum + (size_t)k1 * kM, t, spec_cols);
+    auto twiddle = [&](float2(&x)[kE]) { apply_twiddles_from<kE, -1>(x, first); };
+    auto twiddle_conj = [&](float2(&x)[kE]) { apply_twiddles_from<kE, 1>(x, first); };
+    for (int pulse = cluster; pulse < pulses; pulse += clusters) {
+        if (t < R && pulse + clusters < pulses) {
+            // chunk n1 = t of the slice this CTA reads next: [t M + k1 S, t M + k1 S + S) within
+            // the row's `avail` samples, whole 16-byte words of a 16-byte aligned row only
+            const float2* nx = src.row(pulse + clusters);
+            const int lo = t * kM + k1 * S;
+            const int hi = (lo + S < avail ? lo + S : avail) & ~1;
+            if (hi > lo && (reinterpret_cast<uintptr_t>(nx) & 15) == 0)
+                bulk_prefetch_l2(nx + lo, (uint32_t)(hi - lo) * (uint32_t)sizeof(float2));
+        }
+        const float2* xr = src.row(pulse);
+        cross_dif_scatter<R, -1>(cl, sm, k1, t, tw,
+                                 [&](int e) { return e < avail ? __ldcs(&xr[e]) : make_float2(0.f, 0.f); });
+        float2 v[kE];
+        take_own(v, sm, t);
+        local_fft_forward<LP>(v, sm, t, twiddle, tab);
+        tmem_multiply<kE, false>(v, spec_cols);
+        local_fft_inverse<LP>(v, sm, t, twiddle_conj, tab);
+        cross_dit_gather<R, 1>(cl, v, sm, k1, t, tw, y + (size_t)pulse * N, 1.0f);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, kCols);
+    }
+}
+
 // Batched C2C rows of length N, natural order in and out; forward unnormalised,
 // inverse scaled by 1/N.  Every CTA reads its input slice before the second cluster
 // barrier and writes only after later ones, so x == y is safe.
@@ -295,10 +375,57 @@ int replica_long(const float2* h, int length, int normalize, int kind, const flo
     return ZKX_SUCCESS;
 }
 
+constexpr size_t kLocalSmemBytes =
+    ((size_t)LocalPlan<kM>::EXCHANGE + 2 + LocalPlan<kM>::TABLE + (size_t)kT * (ilog2(kE) | 1)) * sizeof(float2);
+
+// Clusters of the persistent kernel resident on the GPU at once.
+template <int R>
+int local_long_clusters(int* clusters)
+{
+    auto k = long_compression_local_kernel<R, RowsContiguous>;
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLocalSmemBytes));
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(R);
+    cfg.blockDim = dim3(kT);
+    cfg.dynamicSmemBytes = kLocalSmemBytes;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = R;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    ZKX_CUDA(cudaOccupancyMaxActiveClusters(clusters, k, &cfg));
+    *clusters = std::max(1, *clusters);
+    return ZKX_SUCCESS;
+}
+
+// The default: the persistent kernel once every resident cluster gets at least four pulses,
+// one cluster per pulse below that (measured chain times: 2048 x 65536 2940 vs 3120 us,
+// 512 x 32768 324 vs 329 us; 64 x 65536 114 vs 106 us, 256 x 32768 192 vs 189 us).
+int long_default_variant(int pulses, int clusters)
+{
+    return pulses >= 4 * clusters ? ZKX_COMPRESSION_LOCAL : ZKX_COMPRESSION_PERSISTENT;
+}
+
 template <int R, class Src>
 int compression_long(const Src& x, int pulses, int samples, const float2* spectrum, float2* y,
-                     cudaStream_t s)
+                     int variant, cudaStream_t s)
 {
+    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
+    int clusters = 1;
+    if (variant == ZKX_COMPRESSION_DEFAULT || variant == ZKX_COMPRESSION_LOCAL) {
+        ZKX_TRY(local_long_clusters<R>(&clusters));
+        if (variant == ZKX_COMPRESSION_DEFAULT) variant = long_default_variant(pulses, clusters);
+    }
+    if (variant == ZKX_COMPRESSION_LOCAL) {
+        auto k = long_compression_local_kernel<R, Src>;
+        ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLocalSmemBytes));
+        clusters = std::max(1, std::min(pulses, clusters));
+        k<<<(unsigned)clusters * R, kT, kLocalSmemBytes, s>>>(x, pulses, samples, spectrum, y, twiddle_table());
+        ZKX_LAUNCHED("long_compression_local_kernel");
+        return ZKX_SUCCESS;
+    }
     auto k = long_compression_kernel<R, Src>;
     ZKX_TRY(prepare(k));
     int dev = 0, sms = 0;
@@ -335,23 +462,33 @@ int launch_long_replica_spectrum(const float2* replica, int length, int nfft, in
 
 template <class Src>
 int long_compression(const Src& x, int pulses, int samples, int nfft, const float2* spectrum,
-                     float2* y, cudaStream_t stream)
+                     float2* y, int variant, cudaStream_t stream)
 {
-    if (nfft == 2 * kM) return compression_long<2>(x, pulses, samples, spectrum, y, stream);
-    if (nfft == 4 * kM) return compression_long<4>(x, pulses, samples, spectrum, y, stream);
+    if (nfft == 2 * kM) return compression_long<2>(x, pulses, samples, spectrum, y, variant, stream);
+    if (nfft == 4 * kM) return compression_long<4>(x, pulses, samples, spectrum, y, variant, stream);
     return unsupported();
 }
 
-int launch_long_compression(const RowsContiguous& x, int pulses, int samples, int nfft,
-                            const float2* spectrum, float2* y, cudaStream_t stream)
+int resolve_long_compression_variant(int pulses, int nfft, int* resolved)
 {
-    return long_compression(x, pulses, samples, nfft, spectrum, y, stream);
+    int clusters = 1;
+    if (nfft == 2 * kM) ZKX_TRY(local_long_clusters<2>(&clusters));
+    else if (nfft == 4 * kM) ZKX_TRY(local_long_clusters<4>(&clusters));
+    else return unsupported();
+    *resolved = long_default_variant(pulses, clusters);
+    return ZKX_SUCCESS;
+}
+
+int launch_long_compression(const RowsContiguous& x, int pulses, int samples, int nfft,
+                            const float2* spectrum, float2* y, int variant, cudaStream_t stream)
+{
+    return long_compression(x, pulses, samples, nfft, spectrum, y, variant, stream);
 }
 
 int launch_long_compression(const RowsTable& x, int pulses, int samples, int nfft,
-                            const float2* spectrum, float2* y, cudaStream_t stream)
+                            const float2* spectrum, float2* y, int variant, cudaStream_t stream)
 {
-    return long_compression(x, pulses, samples, nfft, spectrum, y, stream);
+    return long_compression(x, pulses, samples, nfft, spectrum, y, variant, stream);
 }
 
 int launch_long_fft_rows(const float2* x, int rows, int n, int inverse, float2* y,

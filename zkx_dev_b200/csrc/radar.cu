@@ -225,23 +225,6 @@ constexpr int local_tmem_columns()
     return c < 32 ? 32 : c;
 }
 
-// v[k] *= s_k (CONJ: conj(s_k)) with s_k the complex word pair at columns 2k, 2k+1.
-template <int E, bool CONJ>
-__device__ __forceinline__ void tmem_multiply(float2 (&v)[E], uint32_t cols)
-{
-#pragma unroll
-    for (int c = 0; c < 2 * E; c += 16) {
-        float w[16];
-        tmem_load16(cols + c, w);
-        tmem_wait_load();
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const float2 m = make_float2(w[2 * i], w[2 * i + 1]);
-            v[c / 2 + i] = CONJ ? cmulc(v[c / 2 + i], m) : cmul(v[c / 2 + i], m);
-        }
-    }
-}
-
 template <int N, class Src>
 __global__ void __launch_bounds__(LocalPlan<N>::T)
 pulse_compression_local_kernel(const Src src, int pulses, int samples, const float2* __restrict__ spectrum,
@@ -276,19 +259,7 @@ pulse_compression_local_kernel(const Src src, int pulses, int samples, const flo
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
     const uint32_t spec_cols = tmem_base + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(warp >> 2) * (2 * LP::E);
-    // this thread's spectrum bins, in register order, into its tensor-memory lane
-#pragma unroll
-    for (int c = 0; c < 2 * LP::E; c += 16) {
-        float sv[16];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const float2 b = __ldg(&spectrum[local_bin<LP>(t, c / 2 + i)]);
-            sv[2 * i] = b.x;
-            sv[2 * i + 1] = b.y;
-        }
-        tmem_store16(spec_cols + c, sv);
-    }
-    tmem_wait_store();
+    spectrum_to_tmem<LP>(spectrum, t, spec_cols);
     auto twiddle = [&](float2(&x)[LP::E]) { apply_twiddles_from<LP::E, -1>(x, first); };
     auto twiddle_conj = [&](float2(&x)[LP::E]) { apply_twiddles_from<LP::E, 1>(x, first); };
 
@@ -742,7 +713,7 @@ int launch_pulse_compression_variant(const float2* x, int pulses, int samples, i
     const RowsContiguous src{x, samples};
     if (!is_pow2(nfft)) return launch_compression_any(src, pulses, samples, nfft, spectrum, y, stream);
     if (nfft > (1 << kMaxSmemFftLog))
-        return launch_long_compression(src, pulses, samples, nfft, spectrum, y, stream);
+        return launch_long_compression(src, pulses, samples, nfft, spectrum, y, variant, stream);
     const bool aligned16 = (samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0;
 #define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, variant, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
@@ -752,7 +723,10 @@ int launch_pulse_compression_variant(const float2* x, int pulses, int samples, i
 int resolve_compression_variant(int pulses, int nfft, int variant, int* resolved)
 {
     *resolved = variant;
-    if (variant != ZKX_COMPRESSION_DEFAULT || !is_pow2(nfft) || !local_fft_for(nfft)) return ZKX_SUCCESS;
+    if (variant != ZKX_COMPRESSION_DEFAULT || !is_pow2(nfft)) return ZKX_SUCCESS;
+    if (nfft == 2 * (1 << kMaxSmemFftLog) || nfft == 4 * (1 << kMaxSmemFftLog))
+        return resolve_long_compression_variant(pulses, nfft, resolved);
+    if (!local_fft_for(nfft)) return ZKX_SUCCESS;
     int slots = 0;
     switch (nfft) {
     case 4096: ZKX_TRY(local_compression_slots<4096>(&slots)); break;
@@ -780,7 +754,7 @@ int launch_pulse_compression_table(const float2* const* cpis, int count, int pul
     const int pulses = count * pulses_per_cpi;
     if (!is_pow2(nfft)) return launch_compression_any(src, pulses, samples, nfft, spectrum, y, stream);
     if (nfft > (1 << kMaxSmemFftLog))
-        return launch_long_compression(src, pulses, samples, nfft, spectrum, y, stream);
+        return launch_long_compression(src, pulses, samples, nfft, spectrum, y, variant, stream);
 #define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, variant, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
 #undef ZKX_CALL

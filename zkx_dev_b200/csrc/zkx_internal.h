@@ -93,10 +93,13 @@ int launch_fft_rows(const float2* x, int rows, int n, int inverse, float2* y, cu
 int launch_long_replica_spectrum(const float2* replica, int length, int nfft, int normalize,
                                  int window_kind, const float* explicit_window, float2* spectrum,
                                  cudaStream_t stream);
+// The concrete kernel ZKX_COMPRESSION_DEFAULT stands for at `pulses` pulses of a 32768- or
+// 65536-point compression.
+int resolve_long_compression_variant(int pulses, int nfft, int* resolved);
 int launch_long_compression(const RowsContiguous& x, int pulses, int samples, int nfft,
-                            const float2* spectrum, float2* y, cudaStream_t stream);
+                            const float2* spectrum, float2* y, int variant, cudaStream_t stream);
 int launch_long_compression(const RowsTable& x, int pulses, int samples, int nfft,
-                            const float2* spectrum, float2* y, cudaStream_t stream);
+                            const float2* spectrum, float2* y, int variant, cudaStream_t stream);
 // The concrete ZKX_COMPRESSION_* kernel that `variant` stands for at `pulses` pulses of
 // nfft points (ZKX_COMPRESSION_DEFAULT resolves by the four-step kernels' rule; any other
 // value is returned as is).  Plans resolve it once from their per-CPI shape, so a CPI gives
