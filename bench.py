@@ -845,6 +845,26 @@ def reference_cpu_baseline(steps: int, warmup: int, budget_s: float = 90.0,
     return res
 
 
+def profile_shape(shape: str, precision: str = "fp32") -> None:
+    """One warm-up and one run of the chain with the by-shape kernel defaults on a P x N CPI
+    generated on the device (the profiling target for transform lengths the bench workload
+    does not use)."""
+    import torch
+    import zkx_dev_b200 as z
+    from zkx_dev_b200 import synth
+    P_, N_ = (int(v) for v in shape.lower().split("x"))
+    L_ = max(1, N_ // 16)
+    torch.cuda.set_device(0)
+    x = synth.device_cpi(P_, N_, synth.draw_targets(P_, N_, 64, L_, synth.seed_for(5, 7)), L_, synth.seed_for(5, 8))
+    chain = z.RangeDopplerChain(z.ChainConfig(P_, N_, L_, precision=precision),
+                                torch.as_tensor(synth.lfm_chirp(L_).astype(np.complex64), device="cuda"))
+    out = chain.allocate_outputs(keep_rd=False)
+    for _ in range(2):
+        chain(x, out)
+    torch.cuda.synchronize()
+    chain.close()
+
+
 # ------------------------------------------------------------------------ main
 
 def main() -> None:
@@ -861,11 +881,21 @@ def main() -> None:
     ap.add_argument("--profile", action="store_true",
                     help="one input set, one warm-up and one step of every stage, no timing "
                          "(the command profiled under ncu)")
+    ap.add_argument("--shape", default=None,
+                    help="with --profile: PxN runs the chain (compression, Doppler, CFAR) on one device-"
+                         "generated P x N CPI (chirp N/16, 64 targets) instead of the bench workload, "
+                         "one warm-up and one run (the command profiled for other transform lengths)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "tc_f16", "tc_bf16"],
+                    help="with --profile --shape: the range-compression arithmetic of the profiled chain")
     args = ap.parse_args()
     args.warmup = 1 if args.profile else max(3, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.profile and args.shape:
+        profile_shape(args.shape, args.precision)
+        print("profile pass done")
+        return
     if args.serving_only:
         import torch
         dev = torch.device("cuda", 0)
