@@ -134,3 +134,26 @@ def test_cfar_tiles_give_the_fp64_mask(z, P, N, batch):
         assert np.max(np.abs(t2[inside] - t1[inside]) / t1[inside]) <= 2e-6
     from zkx_dev_b200 import _lib
     assert _lib.kernel_status(clear=True) == 0
+
+
+@pytest.mark.parametrize("P,N", [(600, 16384), (2400, 4096)])
+def test_local_variant_output_alignment(z, P, N):
+    """The four-step kernel stores pairs of outputs with 128-bit stores when the output is
+    16-byte aligned and single values otherwise; both give the same bits (the C ABI with an
+    output pointer 8 bytes past a 16-byte boundary)."""
+    from zkx_dev_b200 import _lib as L
+    from zkx_dev_b200.synth import draw_targets, device_cpi, lfm_chirp
+    lib, sh = L.lib(), L.stream_handle()
+    x = device_cpi(P, N, draw_targets(P, N, 8, 256, seed=3), 256, seed=4)
+    rep = torch.as_tensor(lfm_chirp(256).astype(np.complex64)).cuda()
+    spec = torch.empty(N, dtype=torch.complex64, device="cuda")
+    L.check(lib.zkx_replica_spectrum_c64(rep.data_ptr(), 256, N, 1, L.WINDOW_HAMMING, None, spec.data_ptr(), sh))
+    aligned = torch.empty((P, N), dtype=torch.complex64, device="cuda")
+    buf = torch.empty(P * N + 1, dtype=torch.complex64, device="cuda")
+    shifted = buf[1:].view(P, N)
+    assert aligned.data_ptr() % 16 == 0 and shifted.data_ptr() % 16 == 8
+    for y in (aligned, shifted):
+        L.check(lib.zkx_pulse_compression_spectrum_c64(x.data_ptr(), P, N, N, spec.data_ptr(), y.data_ptr(), sh))
+    torch.cuda.synchronize()
+    assert torch.equal(aligned, shifted)
+    assert L.kernel_status(clear=True) == 0

@@ -19,6 +19,8 @@
 // Per pulse the CTA synchronises twice per direction instead of three to four times,
 // and the local exchanges of one warp overlap the arithmetic of the others.
 //
+// The butterflies use scalar complex adds (dft<.., false>), faster here than the packed form.
+//
 // Shared layout: group g owns E * Q words at g * PITCH (Q = P + 1 words per row of the
 // local exchange, an odd pitch that spreads a half-warp's column reads over all banks;
 // PITCH keeps the two groups of a half-warp on disjoint banks when P = 8).  The global
@@ -74,7 +76,7 @@ __device__ __forceinline__ void local_fft_forward(float2 (&v)[LP::E], float2* sm
     const int g = t / P, u = t - (t / P) * P;
     float2* region = sm + g * LP::PITCH;
     // pass 1
-    dft<E, -1>(v);
+    dft<E, -1, false>(v);
     twiddle(v);
     static_for<0, E>([&](auto K) {
         constexpr int k = decltype(K)::value;
@@ -86,7 +88,7 @@ __device__ __forceinline__ void local_fft_forward(float2 (&v)[LP::E], float2* sm
         constexpr int r = decltype(R)::value;
         v[r] = region[u + P * r];
     });
-    dft<E, -1>(v);
+    dft<E, -1, false>(v);
     apply_twiddles_table<E, -1>(v, u, tab);
     __syncwarp();
     static_for<0, E>([&](auto K) {
@@ -99,7 +101,7 @@ __device__ __forceinline__ void local_fft_forward(float2 (&v)[LP::E], float2* sm
         constexpr int j = decltype(JJ)::value;
         float2 z[P];
         static_for<0, P>([&](auto U) { z[decltype(U)::value] = region[(u + P * j) * Q + decltype(U)::value]; });
-        dft<P, -1>(z);
+        dft<P, -1, false>(z);
         static_for<0, P>([&](auto K3) { v[j * P + decltype(K3)::value] = z[decltype(K3)::value]; });
     });
 }
@@ -121,7 +123,7 @@ __device__ __forceinline__ void local_fft_inverse(float2 (&v)[LP::E], float2* sm
         constexpr int j = decltype(JJ)::value;
         float2 z[P];
         static_for<0, P>([&](auto K3) { z[decltype(K3)::value] = v[j * P + decltype(K3)::value]; });
-        dft<P, 1>(z);
+        dft<P, 1, false>(z);
         static_for<0, P>([&](auto U) { region[(u + P * j) * Q + decltype(U)::value] = z[decltype(U)::value]; });
     });
     __syncwarp();
@@ -131,7 +133,7 @@ __device__ __forceinline__ void local_fft_inverse(float2 (&v)[LP::E], float2* sm
         v[k] = region[k * Q + u];
     });
     apply_twiddles_table<E, 1>(v, u, tab);
-    dft<E, 1>(v);
+    dft<E, 1, false>(v);
     __syncwarp();
     static_for<0, E>([&](auto R) {
         constexpr int r = decltype(R)::value;
@@ -144,7 +146,7 @@ __device__ __forceinline__ void local_fft_inverse(float2 (&v)[LP::E], float2* sm
         v[k] = sm[k * LP::PITCH + t];
     });
     twiddle_conj(v);
-    dft<E, 1>(v);
+    dft<E, 1, false>(v);
 }
 
 // Spectrum index of register q = j P + k3 of thread t after local_fft_forward.
