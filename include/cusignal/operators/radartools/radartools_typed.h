@@ -18,6 +18,7 @@
 #include <limits>
 #include <stdexcept>
 #include <type_traits>
+#include <atomic>
 #include <vector>
 
 namespace cusignal {
@@ -304,6 +305,32 @@ DeviceArray<double> cfar_alpha_device(T pfa, int reference)
 }
 
 /// CA-CFAR into caller-allocated threshold and detections (same element count as x).
+// How ca_cfar_device evaluates a 2-D map (process-wide; no counterpart in the reference, whose
+// only evaluation is the first):
+//   reference_order  the reference's FP32 integral image in its summation order: thresholds and
+//                    masks bit-identical to ca_cfar_typed_cpu<float>, which is what Task1's
+//                    same-power comparison requires (the default);
+//   fp64_decided     the tiled kernel whose ring sums take no differences of running sums and
+//                    whose near-threshold cells are re-decided in FP64: the mask equals an FP64
+//                    CFAR of the same input, on planes of any size (on large planes the FP32
+//                    integral image loses the threshold where running sums dwarf window sums).
+// Rank-1 inputs always use the reference order.
+enum class CaCfarDeviceMethod { reference_order, fp64_decided };
+
+inline std::atomic<int>& ca_cfar_device_method_slot()
+{
+    static std::atomic<int> method{static_cast<int>(CaCfarDeviceMethod::reference_order)};
+    return method;
+}
+inline void set_ca_cfar_device_method(CaCfarDeviceMethod method)
+{
+    ca_cfar_device_method_slot().store(static_cast<int>(method));
+}
+inline CaCfarDeviceMethod ca_cfar_device_method()
+{
+    return static_cast<CaCfarDeviceMethod>(ca_cfar_device_method_slot().load());
+}
+
 template <class T>
 void ca_cfar_device(const DeviceArray<T>& x, const std::vector<int>& shape, const CaCfarOptions& options,
                     DeviceArray<float>& threshold, DeviceArray<CfarDetection>& detections)
@@ -332,8 +359,10 @@ void ca_cfar_device(const DeviceArray<T>& x, const std::vector<int>& shape, cons
     const int g1 = rank == 2 ? options.guard_cells[1] : 0;
     const int r1 = rank == 2 ? options.reference_cells[1] : 0;
     auto* det = reinterpret_cast<uint8_t*>(detections.data());
+    const int mode = ca_cfar_device_method() == CaCfarDeviceMethod::fp64_decided ? ZKX_CFAR_ACCURATE
+                                                                                : ZKX_CFAR_COMPAT;
     detail::zkx_check(zkx_ca_cfar_f32(xf.data(), rank, rows, cols, options.guard_cells[0], g1,
-                                      options.reference_cells[0], r1, options.pfa, ZKX_CFAR_COMPAT,
+                                      options.reference_cells[0], r1, options.pfa, mode,
                                       threshold.data(), det, nullptr));
     if constexpr (std::is_integral_v<T>)
         detail::zkx_check(zkx_cfar_detect_int(x.data(), detail::zkx_dtype<T>(), threshold.data(),

@@ -443,7 +443,9 @@ enum {
 enum {
     ZKX_CFAR_TILE_DEFAULT = 0,
     ZKX_CFAR_TILE_FULL = 1,    /* 64 x 64 tile, row-sum planes of the whole tile (3 CTAs per SM) */
-    ZKX_CFAR_TILE_HALVES = 2   /* 64 x 64 tile, row-sum planes built in two 32-row halves (4 CTAs per SM) */
+    ZKX_CFAR_TILE_HALVES = 2,  /* 64 x 64 tile, row-sum planes built in two 32-row halves (4 CTAs per SM) */
+    ZKX_CFAR_TILE_STREAM = 3   /* persistent full tiles, two CTAs per SM, next tile's halo copied during
+                                  this one; the default (thresholds equal to ZKX_CFAR_TILE_FULL's) */
 };
 typedef struct {
     int compression_variant;  /* ZKX_COMPRESSION_* */

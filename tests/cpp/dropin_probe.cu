@@ -91,6 +91,10 @@ int main(int argc, char** argv)
         auto cf = ca_cfar_device(dpower, {P, N}, co);
         save("thr", cf.threshold.to_host());
         save("det", cf.detections.to_host());
+        set_ca_cfar_device_method(CaCfarDeviceMethod::fp64_decided);
+        auto cf64 = ca_cfar_device(dpower, {P, N}, co);
+        set_ca_cfar_device_method(CaCfarDeviceMethod::reference_order);
+        save("det64", cf64.detections.to_host());
 
         // integer CFAR input (floor rule) and half-precision compression input
         auto ipow = DeviceArray<std::int16_t>::from_host(load<std::int16_t>("ipow.bin"));

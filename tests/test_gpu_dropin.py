@@ -111,6 +111,9 @@ def test_dropin_api_matches_oracle():
         thr_ref, det_ref = O.ca_cfar_compat(power, (2, 2), (4, 4), 1e-3)
         np.testing.assert_array_equal(out("thr", np.float32).reshape(P, N), thr_ref)
         np.testing.assert_array_equal(out("det", np.uint8).reshape(P, N), det_ref)
+        # opted into the FP64-decided evaluation: the mask of an FP64 CFAR of the same power
+        _, det64 = O.ca_cfar_f64(power, (2, 2), (4, 4), 1e-3)
+        np.testing.assert_array_equal(out("det64", np.uint8).reshape(P, N), det64)
         # the probe passes pfa as float (1e-3f): alpha follows that FP32 probability in FP64
         assert out("alpha", np.float64)[0] == pytest.approx(
             O.cfar_alpha(float(np.float32(1e-3)), 2 * 4 * 13 + 2 * 5 * 4), rel=1e-15)

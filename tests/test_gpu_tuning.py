@@ -53,7 +53,7 @@ def test_autotune_choice_is_valid_and_shared(z):
     chain = z.RangeDopplerChain(z.ChainConfig(P, N, L), rep)
     chosen = chain.autotune(x)
     assert chosen["compression_variant"] in (1, 2, 3) and chosen["doppler_columns"] in (8, 16)
-    assert chosen["cfar_tile"] in (1, 2)
+    assert chosen["cfar_tile"] in (1, 2, 3)
     assert chain.tuning == chosen
     again = z.RangeDopplerChain(z.ChainConfig(P, N, L), rep)
     assert again.tuning == chosen
@@ -107,18 +107,20 @@ def test_local_variant_stacked_batch(z):
         assert torch.equal(batch["detections"][b], alone["detections"])
 
 
-@pytest.mark.parametrize("P,N,batch", [(1024, 16384, 1), (100, 4000, 2), (256, 2048, 3)])
+@pytest.mark.parametrize("P,N,batch", [(1024, 16384, 1), (100, 4000, 2), (256, 2048, 3), (64, 1024, 40)])
 def test_cfar_tiles_give_the_fp64_mask(z, P, N, batch):
-    """Both tiled CA-CFAR kernels (row-sum planes of the whole tile, or built in two 32-row
-    halves) give the FP64 CFAR's mask of the same power, on full and partial tiles and on
-    stacked batches; their thresholds agree to FP32 rounding."""
+    """The tiled CA-CFAR kernels (row-sum planes of the whole tile, built in two 32-row
+    halves, or whole-tile planes in persistent CTAs that walk the tiles of every map) give
+    the FP64 CFAR's mask of the same power, on full and partial tiles and on stacked
+    batches; their thresholds agree to FP32 rounding, and the persistent kernel's equal the
+    whole-tile kernel's bit for bit."""
     import oracle as O
     from zkx_dev_b200.synth import make_cpi
     cpis = [make_cpi(P, N, 10, 64, seed=N + b) for b in range(batch)]
     chain = z.RangeDopplerChain(z.ChainConfig(P, N, 64), torch.as_tensor(cpis[0].replica).cuda())
     x = torch.as_tensor(np.stack([c.x for c in cpis])).cuda()
     outs = {}
-    for tile in (1, 2):
+    for tile in (1, 2, 3):
         set_tuning(chain, 0, 0, tile)
         o = chain.run_batch(x)
         torch.cuda.synchronize()
@@ -127,6 +129,8 @@ def test_cfar_tiles_give_the_fp64_mask(z, P, N, batch):
         _, m64 = O.ca_cfar_f64_bands(outs[2]["power"][b], (2, 2), (8, 8), 1e-6)
         np.testing.assert_array_equal(outs[2]["detections"][b], m64)
         np.testing.assert_array_equal(outs[1]["detections"][b], m64)
+        np.testing.assert_array_equal(outs[3]["detections"][b], m64)
+        np.testing.assert_array_equal(outs[3]["threshold"][b], outs[1]["threshold"][b])
         t1 = outs[1]["threshold"][b].astype(np.float64)
         t2 = outs[2]["threshold"][b].astype(np.float64)
         inside = t1 > 0

@@ -686,7 +686,7 @@ extern "C" int zkx_rd_plan_autotune(zkx_rd_plan p, const void* x, int batch, zkx
             const int* gd = p->d.guard_cells;
             const int* rf = p->d.reference_cells;
             float tbest = 0.f;
-            for (int tile : {ZKX_CFAR_TILE_FULL, ZKX_CFAR_TILE_HALVES}) {
+            for (int tile : {ZKX_CFAR_TILE_FULL, ZKX_CFAR_TILE_HALVES, ZKX_CFAR_TILE_STREAM}) {
                 float ms = 0.f;
                 rc = time_median([&] {
                     return launch_ca_cfar_accurate(power, nd, nr, gd[0], gd[1], rf[0], rf[1], p->cfar.alpha,
@@ -726,7 +726,7 @@ extern "C" int zkx_rd_plan_set_tuning(zkx_rd_plan p, const zkx_rd_tuning* t)
     if (!p || !t) return fail(ZKX_INVALID_ARGUMENT, "rd_plan_set_tuning: null pointer");
     if (t->compression_variant < 0 || t->compression_variant > ZKX_COMPRESSION_LOCAL ||
         (t->doppler_columns != 0 && t->doppler_columns != 8 && t->doppler_columns != 16) ||
-        t->cfar_tile < 0 || t->cfar_tile > ZKX_CFAR_TILE_HALVES)
+        t->cfar_tile < 0 || t->cfar_tile > ZKX_CFAR_TILE_STREAM)
         return fail(ZKX_INVALID_ARGUMENT, "rd_plan_set_tuning: unknown kernel choice");
     p->tuning = *t;
     return ZKX_SUCCESS;

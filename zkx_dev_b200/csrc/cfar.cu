@@ -238,44 +238,17 @@ struct CfarTmaGeom {
     }
 };
 
+// Vertical pieces of a staged 64 x 64 tile: one item per (halo column, 32-row segment), a
+// round of the CTA's threads for the 2/8 window (84 halo columns x 2 segments); longer
+// segments sum fewer halo rows per cell.
 template <int GR, int GC, int RR, int RC>
-__global__ void __launch_bounds__(kCfarThreads, 3)
-cfar_accurate_tma_kernel(const __grid_constant__ CUtensorMap tmap, int rows, int cols,
-                         float scale32, double scale64, float* __restrict__ thr,
-                         uint8_t* __restrict__ det, int* err)
+__device__ __forceinline__ void full_tile_vertical(const float* P, float* SA, float* SB)
 {
     using G = CfarTmaGeom<GR, GC, RR, RC>;
-    constexpr int MR = G::MR, MC = G::MC, HC = G::HC, OFF = G::OFF, BOXW = G::BOXW;
-    constexpr int PITCH = G::PITCH, TY = kCfarTY, TX = kCfarTX;
-    extern __shared__ __align__(128) float csm[];
-    float* P = csm;                           // [HR][BOXW]; halo column hc at P[.. + hc + OFF]
-    float* SA = P + G::HR * BOXW;             // [TY][PITCH]
-    float* SB = SA + TY * PITCH;              // [TY][PITCH]
-    uint64_t* bar = reinterpret_cast<uint64_t*>(SB + TY * PITCH);
-    const int r0 = blockIdx.y * TY;
-    const int c0 = blockIdx.x * TX;
-    // map of a stacked batch: its rows follow the previous map's; halo rows that reach a
-    // neighbouring map only feed border cells, whose threshold is 0
-    const int map_row0 = blockIdx.z * rows;
-    thr += (size_t)blockIdx.z * rows * cols;
-    det += (size_t)blockIdx.z * rows * cols;
-    if (threadIdx.x == 0) mbar_init(bar, 1);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(bar, (uint32_t)(G::HR * BOXW * sizeof(float)));
-        tma_load_2d(P, &tmap, c0 - MC - OFF, map_row0 + r0 - MR, bar);
-    }
-    const bool ok = mbar_wait_bounded(bar, 0);
-    if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
-        return;
-    }
-
-    // 32-row segments: the vertical pass of a 64 x 64 tile is one round of the CTA's threads
-    // (84 halo columns x 2 segments for the 2/8 window) and sums fewer halo rows per cell
+    constexpr int MR = G::MR, HC = G::HC, OFF = G::OFF, BOXW = G::BOXW, PITCH = G::PITCH;
     constexpr int SEG = 32;
     constexpr int VL = SEG + 2 * MR;
-    for (int item = threadIdx.x; item < HC * (TY / SEG); item += kCfarThreads) {
+    for (int item = threadIdx.x; item < HC * (kCfarTY / SEG); item += kCfarThreads) {
         const int seg = item / HC;
         const int hc = item - seg * HC;
         const int rb = seg * SEG;
@@ -291,12 +264,22 @@ cfar_accurate_tma_kernel(const __grid_constant__ CUtensorMap tmap, int rows, int
             SB[(rb + r) * PITCH + hc] = wg[r + MR - GR];
         }
     }
-    __syncthreads();
+}
 
+// Horizontal pass of a staged tile at (r0, c0) of a rows x cols map: thread t owns 16
+// cells of tile row t % 64; writes their thresholds and detections (thr, det point at the
+// map).  Rows below the map are skipped.
+template <int GR, int GC, int RR, int RC>
+__device__ __forceinline__ void full_tile_horizontal(const float* P, const float* SA, const float* SB, int r0,
+                                                     int c0, int rows, int cols, float scale32, double scale64,
+                                                     float* __restrict__ thr, uint8_t* __restrict__ det)
+{
+    using G = CfarTmaGeom<GR, GC, RR, RC>;
+    constexpr int MR = G::MR, MC = G::MC, OFF = G::OFF, BOXW = G::BOXW, PITCH = G::PITCH;
     constexpr int CS = 16;
     constexpr int HL = CS + 2 * MC;
-    const int r = threadIdx.x % TY;
-    const int cb = (threadIdx.x / TY) * CS;
+    const int r = threadIdx.x % kCfarTY;
+    const int cb = (threadIdx.x / kCfarTY) * CS;
     const int grow = r0 + r;
     if (grow >= rows) return;
     float a[HL], b[HL];
@@ -374,6 +357,114 @@ cfar_accurate_tma_kernel(const __grid_constant__ CUtensorMap tmap, int rows, int
 #pragma unroll
         for (int j = 0; j < CS; ++j)
             if (cstart + j < cols) drow[j] = dout[j];
+    }
+}
+
+template <int GR, int GC, int RR, int RC>
+__global__ void __launch_bounds__(kCfarThreads, 3)
+cfar_accurate_tma_kernel(const __grid_constant__ CUtensorMap tmap, int rows, int cols,
+                         float scale32, double scale64, float* __restrict__ thr,
+                         uint8_t* __restrict__ det, int* err)
+{
+    using G = CfarTmaGeom<GR, GC, RR, RC>;
+    constexpr int BOXW = G::BOXW, PITCH = G::PITCH;
+    extern __shared__ __align__(128) float csm[];
+    float* P = csm;                           // [HR][BOXW]; halo column hc at P[.. + hc + OFF]
+    float* SA = P + G::HR * BOXW;             // [TY][PITCH]
+    float* SB = SA + kCfarTY * PITCH;         // [TY][PITCH]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(SB + kCfarTY * PITCH);
+    const int r0 = blockIdx.y * kCfarTY;
+    const int c0 = blockIdx.x * kCfarTX;
+    // map of a stacked batch: its rows follow the previous map's; halo rows that reach a
+    // neighbouring map only feed border cells, whose threshold is 0
+    const int map_row0 = blockIdx.z * rows;
+    thr += (size_t)blockIdx.z * rows * cols;
+    det += (size_t)blockIdx.z * rows * cols;
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(bar, (uint32_t)(G::HR * BOXW * sizeof(float)));
+        tma_load_2d(P, &tmap, c0 - G::MC - G::OFF, map_row0 + r0 - G::MR, bar);
+    }
+    const bool ok = mbar_wait_bounded(bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
+        return;
+    }
+    full_tile_vertical<GR, GC, RR, RC>(P, SA, SB);
+    __syncthreads();
+    full_tile_horizontal<GR, GC, RR, RC>(P, SA, SB, r0, c0, rows, cols, scale32, scale64, thr, det);
+}
+
+// Persistent form of the full-tile kernel: two CTAs per SM walk the tiles (column tile
+// fastest, then row tile, then map) in steps of the grid, with two halo buffers, so the
+// halo copy of the CTA's next tile is in flight during the arithmetic of the current one.
+// Each tile is computed exactly as by cfar_accurate_tma_kernel.
+template <int GR, int GC, int RR, int RC>
+struct CfarStreamGeom {
+    using G = CfarTmaGeom<GR, GC, RR, RC>;
+    static constexpr int HALO = G::HR * G::BOXW;              // floats of one halo copy
+    static constexpr int STRIDE = (HALO + 31) / 32 * 32;       // buffers on 128-byte boundaries
+    static constexpr size_t smem_bytes()
+    {
+        return (size_t)2 * STRIDE * sizeof(float) + (size_t)2 * kCfarTY * G::PITCH * sizeof(float) + 16;
+    }
+};
+
+template <int GR, int GC, int RR, int RC>
+__global__ void __launch_bounds__(kCfarThreads, 2)
+cfar_accurate_stream_kernel(const __grid_constant__ CUtensorMap tmap, int rows, int cols, int tiles_x,
+                            int tiles_y, int batch, float scale32, double scale64, float* __restrict__ thr,
+                            uint8_t* __restrict__ det, int* err)
+{
+    using G = CfarTmaGeom<GR, GC, RR, RC>;
+    using GS = CfarStreamGeom<GR, GC, RR, RC>;
+    extern __shared__ __align__(128) float csm[];
+    // halo buffer b at csm + b * STRIDE
+    float* SA = csm + 2 * GS::STRIDE;         // [TY][PITCH]
+    float* SB = SA + kCfarTY * G::PITCH;      // [TY][PITCH]
+    uint64_t* full = reinterpret_cast<uint64_t*>(SB + kCfarTY * G::PITCH);   // full[0], full[1]
+    const int tiles = tiles_x * tiles_y * batch;
+    const int step = (int)gridDim.x;
+    auto issue = [&](int tile, int b) {
+        const int tx = tile % tiles_x, rest = tile / tiles_x;
+        const int ty = rest % tiles_y, z = rest / tiles_y;
+        mbar_arrive_expect_tx(&full[b], (uint32_t)(GS::HALO * sizeof(float)));
+        tma_load_2d(csm + b * GS::STRIDE, &tmap, tx * kCfarTX - G::MC - G::OFF, z * rows + ty * kCfarTY - G::MR, &full[b]);
+    };
+    if (threadIdx.x == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+    }
+    __syncthreads();
+    const int first = (int)blockIdx.x;
+    if (threadIdx.x == 0) {
+        if (first < tiles) issue(first, 0);
+        if (first + step < tiles) issue(first + step, 1);
+    }
+    int k = 0;
+    for (int tile = first; tile < tiles; tile += step, ++k) {
+        const int b = k & 1;
+        const bool ok = mbar_wait_bounded(&full[b], (uint32_t)((k >> 1) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                atomicCAS(err, 0, (int)kKernelTmaTimeout);
+                // the copy that timed out and the one into the other buffer may still be in
+                // flight: wait for them (bounded) before the shared memory is released
+                mbar_wait_bounded(&full[b], (uint32_t)((k >> 1) & 1));
+                if (tile + step < tiles) mbar_wait_bounded(&full[b ^ 1], (uint32_t)(((k + 1) >> 1) & 1));
+            }
+            return;
+        }
+        const int tx = tile % tiles_x, rest = tile / tiles_x;
+        const int ty = rest % tiles_y, z = rest / tiles_y;
+        const float* P = csm + b * GS::STRIDE;
+        full_tile_vertical<GR, GC, RR, RC>(P, SA, SB);
+        __syncthreads();
+        full_tile_horizontal<GR, GC, RR, RC>(P, SA, SB, ty * kCfarTY, tx * kCfarTX, rows, cols, scale32,
+                                             scale64, thr + (size_t)z * rows * cols, det + (size_t)z * rows * cols);
+        __syncthreads();   // halo buffer b, SA and SB are free
+        if (threadIdx.x == 0 && tile + 2 * step < tiles) issue(tile + 2 * step, b);
     }
 }
 
@@ -662,6 +753,22 @@ int accurate_impl(const float* x, int rows, int cols, float s32, double s64, flo
                 ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 k<<<grid, kCfarThreads, smem, s>>>(map, rows, cols, s32, s64, thr, det, kernel_error_word());
                 ZKX_LAUNCHED("cfar_accurate_tma2_kernel");
+                return ZKX_SUCCESS;
+            }
+            if (tile == ZKX_CFAR_TILE_STREAM || tile == ZKX_CFAR_TILE_DEFAULT) {
+                using GS = CfarStreamGeom<GR, GC, RR, RC>;
+                const size_t smem = GS::smem_bytes();
+                auto k = cfar_accurate_stream_kernel<GR, GC, RR, RC>;
+                ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                int dev = 0, sms = 0, per_sm = 0;
+                ZKX_CUDA(cudaGetDevice(&dev));
+                ZKX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+                ZKX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kCfarThreads, smem));
+                const long long tiles = (long long)grid.x * grid.y * grid.z;
+                const int ctas = (int)std::min<long long>(tiles, (long long)sms * std::max(per_sm, 1));
+                k<<<ctas, kCfarThreads, smem, s>>>(map, rows, cols, (int)grid.x, (int)grid.y, batch, s32, s64,
+                                                   thr, det, kernel_error_word());
+                ZKX_LAUNCHED("cfar_accurate_stream_kernel");
                 return ZKX_SUCCESS;
             }
             const size_t smem = G::smem_bytes();
