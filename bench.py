@@ -512,6 +512,48 @@ def run_serving(dev, n_requests: int = 256, pool: int = 24, seconds: float = 2.0
     b.synchronize()
     uneven_graph = reps * n_requests / (a.elapsed_time(b) * 1e-3)
     del graph, stacked
+
+    # (1c) the same requests as one work list: one launch per stage over every (CPI, tile)
+    # entry of every shape (stages the work-list kernels do not take run on their plan's
+    # kernels), captured as one CUDA graph
+    items = []
+    for k in order:
+        ch, _ = chains[cpis[k].x.shape]
+        shp = (ch.doppler_bins, ch.range_bins)
+        items.append((ch, dev_x[k], {"threshold": torch.empty(shp, device=dev),
+                                     "detections": torch.empty(shp, dtype=torch.uint8, device=dev)}))
+    wl = z.WorkList(items)
+    wl_info = wl.info()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        wl.launch()
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        wl.launch()
+    for _ in range(3):
+        graph.replay()
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(reps):
+        graph.replay()
+    b.record()
+    b.synchronize()
+    worklist_graph = reps * n_requests / (a.elapsed_time(b) * 1e-3)
+    # each shape's first request against its CPI alone
+    wl_identical = True
+    seen = set()
+    for (ch, x, o) in items:
+        if ch in seen:
+            continue
+        seen.add(ch)
+        ref = ch.run(x)
+        wl_identical &= bool(torch.equal(ref["detections"], o["detections"]) and
+                             torch.equal(ref["threshold"], o["threshold"]))
+    del graph, items
+    wl.close()
     for ch, _ in chains.values():
         ch.close()
 
@@ -558,6 +600,9 @@ def run_serving(dev, n_requests: int = 256, pool: int = 24, seconds: float = 2.0
         "plain_device_cpis_per_s": round(plain, 1),
         "uneven_graph_cpis_per_s": round(uneven_graph, 1),
         "uneven_graph_shapes": len(groups),
+        "worklist_graph_cpis_per_s": round(worklist_graph, 1),
+        "worklist_launches": wl_info["launches"],
+        "worklist_identical_to_alone": wl_identical,
         "served_device_cpis_per_s": round(st_dev["cpis_per_s"], 1),
         "served_vs_plain_device": round(st_dev["cpis_per_s"] / plain, 3),
         "served_device_gbs": round(st_dev["cpis_per_s"] * cells / n_requests * 45 / 1e9, 1),

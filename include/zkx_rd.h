@@ -451,6 +451,12 @@ typedef struct {
     int compression_variant;  /* ZKX_COMPRESSION_* */
     int doppler_columns;      /* range columns per CTA of the bulk-copy Doppler kernel: 8 or 16 */
     int cfar_tile;            /* ZKX_CFAR_TILE_* (accurate-mode CA-CFAR of the tiled window sizes) */
+    int compression_radix;    /* values per thread (radix plan) of the Stockham compression kernels
+                                 (variants 1, 2): 0 = the plan table's; 16 or 32 where the other
+                                 exists (range nfft 1024 .. 8192; it rounds differently) */
+    int compression_ctas_per_sm;  /* cap on the persistent / four-step compression CTAs per SM (0 = all
+                                     that fit; results unchanged) */
+    int cfar_ctas_per_sm;     /* cap on the persistent CA-CFAR CTAs per SM (0 = all that fit) */
 } zkx_rd_tuning;
 
 /* Times every candidate of each stage on `batch` CPIs at x (device, the plan's shape) on
@@ -471,6 +477,42 @@ ZKX_API int zkx_rd_graph_create(zkx_rd_plan plan, const void* x, int batch, void
                                 zkx_rd_graph* graph);
 ZKX_API int zkx_rd_graph_launch(zkx_rd_graph graph, zkx_stream_t stream);
 ZKX_API int zkx_rd_graph_destroy(zkx_rd_graph graph);
+
+/* ---------------------------------------------------------------- work list
+ * The chain over CPIs of mixed shapes with ONE launch per stage (no counterpart in the
+ * reference, whose Task1 pipeline runs one CPI per call).  create groups the items by
+ * plan, allocates the compressed cubes and power planes of every CPI (grouped by plan,
+ * library-owned) and device tables of the items' pointers, and builds the stage kernels'
+ * parameter blocks; launch enqueues on `stream`
+ *   range compression  one work-list kernel over every (CPI, 512-thread pulse group)
+ *                      entry with a range nfft that is a power of two from 64 to 16384;
+ *   Doppler + |.|^2    one work-list kernel over every (CPI, column tile) entry with a
+ *                      Doppler nfft that is a power of two from 64 to 1024;
+ *   CA-CFAR            one work-list kernel over every (CPI, 64 x 64 tile) entry of the
+ *                      accurate mode with the tiled window geometry of the first such plan;
+ * (at most 24 plans per launch: more plans take one launch per 24).  A plan whose stage
+ * falls outside these (longer or non-power-of-two transforms, a tuning choice that rounds
+ * differently from the work-list kernel, compat mode, another window geometry) runs that
+ * stage with its own kernels, one launch per plan (per CPI for CFAR).  Every CPI's
+ * threshold and detections equal zkx_rd_execute of that CPI alone with its plan, bit for
+ * bit, and so does its power plane, copied to `power` when that is not NULL.  Plans must
+ * have FP32 precision; items must stay valid (and the plans alive) until destroy.  launch
+ * may be captured into a CUDA graph.  count: 1 .. 65535. */
+typedef struct zkx_rd_worklist_s* zkx_rd_worklist;
+typedef struct {
+    zkx_rd_plan plan;
+    const void* x;             /* device complex64 [num_pulses][samples_per_pulse] */
+    float* power;              /* optional device [doppler_bins][range_bins] */
+    float* threshold;          /* device [doppler_bins][range_bins] */
+    uint8_t* detections;       /* device [doppler_bins][range_bins] */
+} zkx_rd_work_item;
+ZKX_API int zkx_rd_worklist_create(const zkx_rd_work_item* items, int count, zkx_rd_worklist* out);
+ZKX_API int zkx_rd_worklist_launch(zkx_rd_worklist list, zkx_stream_t stream);
+/* Launch calls one zkx_rd_worklist_launch makes (a plan's own stage launch of a
+ * non-power-of-two transform or of compat-mode CFAR issues several kernels per call), the
+ * plans (groups), and the library-owned scratch bytes; any pointer may be NULL. */
+ZKX_API int zkx_rd_worklist_info(zkx_rd_worklist list, int* launches, int* groups, long long* scratch_bytes);
+ZKX_API int zkx_rd_worklist_destroy(zkx_rd_worklist list);
 
 /* ---------------------------------------------------------------- serving loop
  * A continuous-batching request loop over the chain (no counterpart in the reference,

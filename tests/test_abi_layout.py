@@ -22,6 +22,7 @@ STRUCTS = {
     "zkx_rd_server_stats": L.ServerStats,
     "zkx_synth_target": L.SynthTarget,
     "zkx_rd_tuning": L.RdTuning,
+    "zkx_rd_work_item": L.WorkItem,
 }
 
 

@@ -54,6 +54,8 @@ def test_autotune_choice_is_valid_and_shared(z):
     chosen = chain.autotune(x)
     assert chosen["compression_variant"] in (1, 2, 3) and chosen["doppler_columns"] in (8, 16)
     assert chosen["cfar_tile"] in (1, 2, 3)
+    assert chosen["compression_radix"] in (0, 16, 32) and chosen["compression_ctas_per_sm"] in (0, 1, 2)
+    assert chosen["cfar_ctas_per_sm"] in (0, 1)
     assert chain.tuning == chosen
     again = z.RangeDopplerChain(z.ChainConfig(P, N, L), rep)
     assert again.tuning == chosen
@@ -161,3 +163,73 @@ def test_local_variant_output_alignment(z, P, N):
     torch.cuda.synchronize()
     assert torch.equal(aligned, shifted)
     assert L.kernel_status(clear=True) == 0
+
+
+def set_full_tuning(chain, **kw):
+    from zkx_dev_b200 import _lib as L
+    t = L.RdTuning(**kw)
+    L.check(L.lib().zkx_rd_plan_set_tuning(chain._plan, ctypes.byref(t)))
+
+
+@pytest.mark.parametrize("P,N,L", [(256, 1024, 64), (128, 2048, 128), (96, 4096, 256), (64, 8192, 512)])
+def test_radix_plan_matches_fp64(z, P, N, L):
+    """The other radix plan of the Stockham compression kernels (16 <-> 32 values per
+    thread) rounds differently: compressed pulses against the FP64 oracle and within FP32
+    rounding of the table's plan, a mask equal to the FP64 CFAR of its power, and each CPI
+    of a stacked batch equal to the CPI alone."""
+    import oracle as O
+    from zkx_dev_b200.synth import make_cpi
+    cpis = [make_cpi(P, N, 8, L, seed=P * 7 + N + b) for b in range(2)]
+    chain = z.RangeDopplerChain(z.ChainConfig(P, N, L), torch.as_tensor(cpis[0].replica).cuda())
+    x = torch.as_tensor(cpis[0].x).cuda()
+    for variant in (1, 2):
+        set_full_tuning(chain, compression_variant=variant)
+        ref = {k: v.clone() for k, v in chain(x).items()}
+        alt = 16 if N in (1024, 8192) else 32
+        set_full_tuning(chain, compression_variant=variant, compression_radix=alt)
+        got = {k: v.clone() for k, v in chain(x).items()}
+        torch.cuda.synchronize()
+        comp = got["compressed"].cpu().numpy().astype(np.complex128)
+        comp2 = ref["compressed"].cpu().numpy().astype(np.complex128)
+        assert np.linalg.norm(comp - comp2) / np.linalg.norm(comp2) <= 1e-6
+        rows = [0, P // 2, P - 1]
+        c64 = O.pulse_compression_fft64(cpis[0].x[rows], cpis[0].replica, -1, True, O.radar_window_f32("hamming", L))
+        assert np.linalg.norm(comp[rows] - c64) / np.linalg.norm(c64) <= 1e-5
+        _, m64 = O.ca_cfar_f64(got["power"].cpu().numpy(), (2, 2), (8, 8), 1e-6)
+        np.testing.assert_array_equal(got["detections"].cpu().numpy(), m64)
+        batch = chain.run_batch(torch.as_tensor(np.stack([c.x for c in cpis])).cuda())
+        torch.cuda.synchronize()
+        assert torch.equal(batch["compressed"][0], got["compressed"])
+        assert torch.equal(batch["detections"][0], got["detections"])
+    from zkx_dev_b200 import _lib
+    assert _lib.kernel_status(clear=True) == 0
+
+
+@pytest.mark.parametrize("P,N,L,variant", [(512, 8192, 512, 2), (1024, 4096, 256, 3), (600, 16384, 1024, 3)])
+def test_cta_caps_do_not_change_results(z, P, N, L, variant):
+    """Capping the persistent compression and CA-CFAR kernels at 1 or 2 CTAs per SM only
+    changes how the pulses and tiles are spread: the results are the same bits."""
+    from zkx_dev_b200.synth import make_cpi
+    cpi = make_cpi(P, N, 10, L, seed=N + variant)
+    chain = z.RangeDopplerChain(z.ChainConfig(P, N, L), torch.as_tensor(cpi.replica).cuda())
+    x = torch.as_tensor(cpi.x).cuda()
+    set_full_tuning(chain, compression_variant=variant, cfar_tile=3)
+    ref = {k: v.clone() for k, v in chain(x).items()}
+    for k in (1, 2):
+        set_full_tuning(chain, compression_variant=variant, cfar_tile=3, compression_ctas_per_sm=k,
+                        cfar_ctas_per_sm=k)
+        got = chain(x)
+        torch.cuda.synchronize()
+        for key in ("compressed", "power", "threshold", "detections"):
+            assert torch.equal(got[key], ref[key]), (k, key)
+
+
+def test_tuning_rejects_unknown_choices(z):
+    from zkx_dev_b200 import _lib as L
+    from zkx_dev_b200.synth import make_cpi
+    cpi = make_cpi(64, 1024, 4, 64, seed=3)
+    chain = z.RangeDopplerChain(z.ChainConfig(64, 1024, 64), torch.as_tensor(cpi.replica).cuda())
+    for kw in ({"compression_radix": 8}, {"compression_ctas_per_sm": -1}, {"cfar_ctas_per_sm": 64},
+               {"cfar_tile": 4}, {"compression_variant": 4}):
+        t = L.RdTuning(**kw)
+        assert L.lib().zkx_rd_plan_set_tuning(chain._plan, ctypes.byref(t)) == L.INVALID_ARGUMENT

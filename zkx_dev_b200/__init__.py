@@ -8,9 +8,9 @@ from ._lib import ZkxError, ZkxValueError, lib
 from .radartools import (ambgfun, ca_cfar, cfar_alpha, fft, pulse_compression, pulse_doppler,
                          replica_spectrum)
 from .filtering import firfilter, firfilter2, hilbert, resample_poly, resample_poly_taps, upfirdn
-from .chain import ChainConfig, RangeDopplerChain
+from .chain import ChainConfig, RangeDopplerChain, WorkList
 from .serving import RdServer, ServerConfig
 
 __all__ = ["ZkxError", "ZkxValueError", "lib", "ambgfun", "ca_cfar", "cfar_alpha", "fft", "pulse_compression",
            "pulse_doppler", "replica_spectrum", "firfilter", "firfilter2", "hilbert", "resample_poly",
-           "resample_poly_taps", "upfirdn", "ChainConfig", "RangeDopplerChain", "RdServer", "ServerConfig"]
+           "resample_poly_taps", "upfirdn", "ChainConfig", "RangeDopplerChain", "WorkList", "RdServer", "ServerConfig"]

@@ -38,6 +38,12 @@ class ResampleLayout(ctypes.Structure):
                 ("output_start", _I)]
 
 
+class WorkItem(ctypes.Structure):
+    """zkx_rd_work_item"""
+    _fields_ = [("plan", ctypes.c_void_p), ("x", ctypes.c_void_p), ("power", ctypes.c_void_p),
+                ("threshold", ctypes.c_void_p), ("detections", ctypes.c_void_p)]
+
+
 class RdDesc(ctypes.Structure):
     _fields_ = [("num_pulses", _I), ("samples_per_pulse", _I), ("range_nfft", _I),
                 ("doppler_nfft", _I), ("replica_length", _I), ("normalize", _I),
@@ -46,7 +52,8 @@ class RdDesc(ctypes.Structure):
 
 
 class RdTuning(ctypes.Structure):
-    _fields_ = [("compression_variant", _I), ("doppler_columns", _I), ("cfar_tile", _I)]
+    _fields_ = [("compression_variant", _I), ("doppler_columns", _I), ("cfar_tile", _I),
+                ("compression_radix", _I), ("compression_ctas_per_sm", _I), ("cfar_ctas_per_sm", _I)]
 
 
 class ServerDesc(ctypes.Structure):
@@ -120,6 +127,10 @@ SIGNATURES = {
     "zkx_rd_graph_create": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, ctypes.POINTER(_P)]),
     "zkx_rd_graph_launch": (_I, [_P, _P]),
     "zkx_rd_graph_destroy": (_I, [_P]),
+    "zkx_rd_worklist_create": (_I, [ctypes.POINTER(WorkItem), _I, ctypes.POINTER(_P)]),
+    "zkx_rd_worklist_launch": (_I, [_P, _P]),
+    "zkx_rd_worklist_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_longlong)]),
+    "zkx_rd_worklist_destroy": (_I, [_P]),
     "zkx_rd_plan_autotune": (_I, [_P, _P, _I, _P, ctypes.POINTER(RdTuning)]),
     "zkx_rd_plan_get_tuning": (_I, [_P, ctypes.POINTER(RdTuning)]),
     "zkx_rd_plan_set_tuning": (_I, [_P, ctypes.POINTER(RdTuning)]),

@@ -132,15 +132,13 @@ class RangeDopplerChain:
         t = L.RdTuning()
         L.check(L.lib().zkx_rd_plan_autotune(self._plan, x.data_ptr(), batch, L.stream_handle(),
                                              ctypes.byref(t)))
-        return {"compression_variant": t.compression_variant, "doppler_columns": t.doppler_columns,
-                "cfar_tile": t.cfar_tile}
+        return {name: getattr(t, name) for name, _ in L.RdTuning._fields_}
 
     @property
     def tuning(self) -> Dict[str, int]:
         t = L.RdTuning()
         L.check(L.lib().zkx_rd_plan_get_tuning(self._plan, ctypes.byref(t)))
-        return {"compression_variant": t.compression_variant, "doppler_columns": t.doppler_columns,
-                "cfar_tile": t.cfar_tile}
+        return {name: getattr(t, name) for name, _ in L.RdTuning._fields_}
 
     def close(self) -> None:
         if getattr(self, "_plan", None) is not None and self._plan.value:
@@ -168,6 +166,64 @@ class ChainGraph:
         if self._g is not None and self._g.value:
             L.lib().zkx_rd_graph_destroy(self._g)
             self._g = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class WorkList:
+    """The chain over CPIs of mixed shapes, one launch per stage (zkx_rd_worklist_*).
+
+    ``items`` is a sequence of ``(chain, x, outputs)``: a RangeDopplerChain (its plan gives
+    the CPI's shape and parameters), the device input CPI and a dict with device
+    ``threshold`` and ``detections`` planes and optionally ``power``.  Each CPI's outputs
+    equal ``chain.run(x)``'s bit for bit.  The tensors must stay alive while the list is
+    used; ``launch`` runs on the current stream and may be captured in a CUDA graph."""
+
+    def __init__(self, items):
+        arr = (L.WorkItem * len(items))()
+        keep = []
+        for i, (chain, x, out) in enumerate(items):
+            P, N = chain.cfg.num_pulses, chain.cfg.samples_per_pulse
+            shape = (chain.doppler_bins, chain.range_bins)
+            x = _complex_input(x, 2, "x")
+            if tuple(x.shape) != (P, N):
+                raise ValueError(f"work item {i}: x must be {P} x {N}")
+            for key, dtype in (("threshold", torch.float32), ("detections", torch.uint8), ("power", torch.float32)):
+                t = out.get(key)
+                if t is None:
+                    if key != "power":
+                        raise ValueError(f"work item {i}: {key} is required")
+                    continue
+                if tuple(t.shape) != shape or t.dtype != dtype or not t.is_contiguous() or not t.is_cuda:
+                    raise ValueError(f"work item {i}: {key} must be a contiguous device {dtype} {shape}")
+            arr[i].plan = chain._plan.value
+            arr[i].x = x.data_ptr()
+            arr[i].threshold = out["threshold"].data_ptr()
+            arr[i].detections = out["detections"].data_ptr()
+            arr[i].power = out["power"].data_ptr() if out.get("power") is not None else None
+            keep.append((chain, x, out))
+        h = ctypes.c_void_p()
+        L.check(L.lib().zkx_rd_worklist_create(arr, len(items), ctypes.byref(h)))
+        self._h = h
+        self._keep = keep
+
+    def launch(self) -> None:
+        L.check(L.lib().zkx_rd_worklist_launch(self._h, L.stream_handle()))
+
+    def info(self) -> Dict[str, int]:
+        launches, groups, scratch = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        L.check(L.lib().zkx_rd_worklist_info(self._h, ctypes.byref(launches), ctypes.byref(groups),
+                                             ctypes.byref(scratch)))
+        return {"launches": launches.value, "groups": groups.value, "scratch_bytes": scratch.value}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            L.lib().zkx_rd_worklist_destroy(self._h)
+            self._h = ctypes.c_void_p()
 
     def __del__(self):
         try:

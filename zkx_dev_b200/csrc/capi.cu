@@ -557,10 +557,12 @@ int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compresse
     } else if (table)
         ZKX_TRY(launch_pulse_compression_table(reinterpret_cast<const float2* const*>(table), batch, P,
                                                N, nr, p->spectrum, static_cast<float2*>(compressed),
-                                               variant, stream));
+                                               variant, stream, p->tuning.compression_radix,
+                                               p->tuning.compression_ctas_per_sm));
     else
         ZKX_TRY(launch_pulse_compression_variant(static_cast<const float2*>(x), batch * P, N, nr, p->spectrum,
-                                                 static_cast<float2*>(compressed), variant, stream));
+                                                 static_cast<float2*>(compressed), variant, stream,
+                                                 p->tuning.compression_radix, p->tuning.compression_ctas_per_sm));
     ZKX_TRY(launch_pulse_doppler(static_cast<const float2*>(compressed), P, nr, nd, p->doppler_window,
                                  static_cast<float2*>(rd), power, batch, p->tuning.doppler_columns, stream));
     const int* gd = p->d.guard_cells;
@@ -574,7 +576,25 @@ int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compresse
         return ZKX_SUCCESS;
     }
     return launch_ca_cfar_accurate(power, nd, nr, gd[0], gd[1], rf[0], rf[1], p->cfar.alpha,
-                                   p->cfar.nref, threshold, detections, batch, p->tuning.cfar_tile, stream);
+                                   p->cfar.nref, threshold, detections, batch, p->tuning.cfar_tile, stream,
+                                   p->tuning.cfar_ctas_per_sm);
+}
+}  // namespace zkx
+
+namespace zkx {
+int rd_plan_view(zkx_rd_plan p, RdPlanView* v)
+{
+    if (!p || !v) return fail(ZKX_INVALID_ARGUMENT, "null plan");
+    v->d = p->d;
+    v->range_nfft = p->range_nfft;
+    v->doppler_nfft = p->doppler_nfft;
+    v->spectrum = p->spectrum;
+    v->doppler_window = p->doppler_window;
+    v->cumulative = p->cumulative;
+    v->alpha = p->cfar.alpha;
+    v->nref = p->cfar.nref;
+    v->tuning = p->tuning;
+    return ZKX_SUCCESS;
 }
 }  // namespace zkx
 
@@ -646,17 +666,44 @@ extern "C" int zkx_rd_plan_autotune(zkx_rd_plan p, const void* x, int batch, zkx
     zkx_rd_tuning best = p->tuning;
     int rc = ZKX_SUCCESS;
     if (p->d.precision == ZKX_PRECISION_FP32) {
+        auto time_compression = [&](int v, int radix, int ctas, float* ms) {
+            return time_median([&] {
+                return launch_pulse_compression_variant(static_cast<const float2*>(x), batch * P, N, nr,
+                                                        p->spectrum, comp, v, stream, radix, ctas);
+            }, stream, ms);
+        };
+        // the kernel, then the radix plan of the Stockham kernels, then the CTAs per SM of
+        // the persistent ones
         float tbest = 0.f;
+        best.compression_radix = 0;
+        best.compression_ctas_per_sm = 0;
         for (int v : {ZKX_COMPRESSION_PLAIN, ZKX_COMPRESSION_PERSISTENT, ZKX_COMPRESSION_LOCAL}) {
             float ms = 0.f;
-            rc = time_median([&] {
-                return launch_pulse_compression_variant(static_cast<const float2*>(x), batch * P, N, nr,
-                                                        p->spectrum, comp, v, stream);
-            }, stream, &ms);
+            rc = time_compression(v, 0, 0, &ms);
             if (rc != ZKX_SUCCESS) break;
             if (v == ZKX_COMPRESSION_PLAIN || ms < tbest) {
                 tbest = ms;
                 best.compression_variant = v;
+            }
+        }
+        const int alt = compression_alt_radix(nr);
+        if (rc == ZKX_SUCCESS && alt != 0 && best.compression_variant != ZKX_COMPRESSION_LOCAL) {
+            float ms = 0.f;
+            rc = time_compression(best.compression_variant, alt, 0, &ms);
+            if (rc == ZKX_SUCCESS && ms < tbest) {
+                tbest = ms;
+                best.compression_radix = alt;
+            }
+        }
+        if (is_pow2(nr) && nr <= 16384 && best.compression_variant != ZKX_COMPRESSION_PLAIN) {
+            for (int k : {1, 2}) {
+                if (rc != ZKX_SUCCESS) break;
+                float ms = 0.f;
+                rc = time_compression(best.compression_variant, best.compression_radix, k, &ms);
+                if (rc == ZKX_SUCCESS && ms < tbest) {
+                    tbest = ms;
+                    best.compression_ctas_per_sm = k;
+                }
             }
         }
     }
@@ -698,6 +745,15 @@ extern "C" int zkx_rd_plan_autotune(zkx_rd_plan p, const void* x, int batch, zkx
                     best.cfar_tile = tile;
                 }
             }
+            best.cfar_ctas_per_sm = 0;
+            if (rc == ZKX_SUCCESS && best.cfar_tile == ZKX_CFAR_TILE_STREAM) {
+                float ms = 0.f;
+                rc = time_median([&] {
+                    return launch_ca_cfar_accurate(power, nd, nr, gd[0], gd[1], rf[0], rf[1], p->cfar.alpha,
+                                                   p->cfar.nref, thr, det, batch, ZKX_CFAR_TILE_STREAM, stream, 1);
+                }, stream, &ms);
+                if (rc == ZKX_SUCCESS && ms < tbest) best.cfar_ctas_per_sm = 1;
+            }
         }
         cudaFree(thr);
         cudaFree(det);
@@ -726,7 +782,10 @@ extern "C" int zkx_rd_plan_set_tuning(zkx_rd_plan p, const zkx_rd_tuning* t)
     if (!p || !t) return fail(ZKX_INVALID_ARGUMENT, "rd_plan_set_tuning: null pointer");
     if (t->compression_variant < 0 || t->compression_variant > ZKX_COMPRESSION_LOCAL ||
         (t->doppler_columns != 0 && t->doppler_columns != 8 && t->doppler_columns != 16) ||
-        t->cfar_tile < 0 || t->cfar_tile > ZKX_CFAR_TILE_STREAM)
+        t->cfar_tile < 0 || t->cfar_tile > ZKX_CFAR_TILE_STREAM ||
+        (t->compression_radix != 0 && t->compression_radix != 16 && t->compression_radix != 32) ||
+        t->compression_ctas_per_sm < 0 || t->compression_ctas_per_sm > 32 || t->cfar_ctas_per_sm < 0 ||
+        t->cfar_ctas_per_sm > 32)
         return fail(ZKX_INVALID_ARGUMENT, "rd_plan_set_tuning: unknown kernel choice");
     p->tuning = *t;
     return ZKX_SUCCESS;

@@ -24,6 +24,7 @@
 #include "fft_core.cuh"
 #include "tma.cuh"
 #include "zkx_internal.h"
+#include "worklist.h"
 
 namespace zkx {
 namespace {
@@ -613,6 +614,64 @@ cfar_accurate_tma2_kernel(const __grid_constant__ CUtensorMap tmap, int rows, in
     }
 }
 
+// CA-CFAR of every map of a work list, whatever its shape: one CTA per (group, map, 64 x 64
+// tile) entry, computed exactly as by cfar_accurate_tma_kernel (whose thresholds the
+// persistent kernel also reproduces); each map writes its own threshold and detection
+// planes.
+template <int GR, int GC, int RR, int RC>
+__global__ void __launch_bounds__(kCfarThreads, 2)
+cfar_worklist_kernel(const __grid_constant__ WlCfarParams p, int* err)
+{
+    using G = CfarTmaGeom<GR, GC, RR, RC>;
+    extern __shared__ __align__(128) float csm[];
+    float* P = csm;                           // [HR][BOXW]
+    float* SA = P + G::HR * G::BOXW;          // [TY][PITCH]
+    float* SB = SA + kCfarTY * G::PITCH;      // [TY][PITCH]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(SB + kCfarTY * G::PITCH);
+    int gi = 0;
+    while (gi + 1 < p.groups && (int)blockIdx.x >= p.g[gi + 1].entry0) ++gi;
+    const WlCfarGroup& W = p.g[gi];
+    const int local = (int)blockIdx.x - W.entry0;
+    const int tx = local % W.tiles_x, rest = local / W.tiles_x;
+    const int ty = rest % W.tiles_y, b = rest / W.tiles_y;
+    const int r0 = ty * kCfarTY, c0 = tx * kCfarTX;
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(bar, (uint32_t)(G::HR * G::BOXW * sizeof(float)));
+        tma_load_2d(P, &W.map, c0 - G::MC - G::OFF, b * W.rows + r0 - G::MR, bar);
+    }
+    const bool ok = mbar_wait_bounded(bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
+        return;
+    }
+    full_tile_vertical<GR, GC, RR, RC>(P, SA, SB);
+    __syncthreads();
+    full_tile_horizontal<GR, GC, RR, RC>(P, SA, SB, r0, c0, W.rows, W.cols, W.scale32, W.scale64, W.thr[b],
+                                         W.det[b]);
+}
+
+template <int GR, int GC, int RR, int RC>
+int cfar_worklist_impl(const WlCfarParams& p, int ctas, cudaStream_t s)
+{
+    using G = CfarTmaGeom<GR, GC, RR, RC>;
+    const size_t smem = G::smem_bytes();
+    auto k = cfar_worklist_kernel<GR, GC, RR, RC>;
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<ctas, kCfarThreads, smem, s>>>(p, kernel_error_word());
+    ZKX_LAUNCHED("cfar_worklist_kernel");
+    return ZKX_SUCCESS;
+}
+
+template <int GR, int GC, int RR, int RC>
+void cfar_box(uint32_t* w, uint32_t* h)
+{
+    using G = CfarTmaGeom<GR, GC, RR, RC>;
+    *w = (uint32_t)G::BOXW;
+    *h = (uint32_t)G::HR;
+}
+
 // Any window geometry: one thread per cell, ring summed directly in FP64.
 __global__ void cfar_generic_kernel(const float* __restrict__ x, int rows, int cols, int gr, int gc,
                                     int rr, int rc, double scale64, float* __restrict__ thr,
@@ -738,7 +797,7 @@ __global__ void compat_threshold_kernel(const float* __restrict__ x, const float
 
 template <int GR, int GC, int RR, int RC>
 int accurate_impl(const float* x, int rows, int cols, float s32, double s64, float* thr,
-                  uint8_t* det, int batch, int tile, cudaStream_t s)
+                  uint8_t* det, int batch, int tile, int ctas_per_sm, cudaStream_t s)
 {
     dim3 grid((cols + kCfarTX - 1) / kCfarTX, (rows + kCfarTY - 1) / kCfarTY, batch);
     using G = CfarTmaGeom<GR, GC, RR, RC>;
@@ -764,8 +823,10 @@ int accurate_impl(const float* x, int rows, int cols, float s32, double s64, flo
                 ZKX_CUDA(cudaGetDevice(&dev));
                 ZKX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
                 ZKX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kCfarThreads, smem));
+                per_sm = std::max(per_sm, 1);
+                if (ctas_per_sm > 0) per_sm = std::min(per_sm, ctas_per_sm);
                 const long long tiles = (long long)grid.x * grid.y * grid.z;
-                const int ctas = (int)std::min<long long>(tiles, (long long)sms * std::max(per_sm, 1));
+                const int ctas = (int)std::min<long long>(tiles, (long long)sms * per_sm);
                 k<<<ctas, kCfarThreads, smem, s>>>(map, rows, cols, (int)grid.x, (int)grid.y, batch, s32, s64,
                                                    thr, det, kernel_error_word());
                 ZKX_LAUNCHED("cfar_accurate_stream_kernel");
@@ -793,13 +854,13 @@ int accurate_impl(const float* x, int rows, int cols, float s32, double s64, flo
 
 int launch_ca_cfar_accurate(const float* x, int rows, int columns, int gr, int gc, int rr, int rc,
                             double alpha, int nref, float* threshold, uint8_t* detections,
-                            int batch, int tile, cudaStream_t stream)
+                            int batch, int tile, cudaStream_t stream, int ctas_per_sm)
 {
     if (batch < 1 || batch > 65535) return fail(ZKX_UNSUPPORTED_OPERATION, "ca_cfar: batch must be 1..65535");
     const double s64 = alpha / (double)nref;
     const float s32 = (float)s64;
 #define ZKX_CFAR_CASE(A, B, C, D) \
-    if (gr == A && gc == B && rr == C && rc == D) return accurate_impl<A, B, C, D>(x, rows, columns, s32, s64, threshold, detections, batch, tile, stream);
+    if (gr == A && gc == B && rr == C && rc == D) return accurate_impl<A, B, C, D>(x, rows, columns, s32, s64, threshold, detections, batch, tile, ctas_per_sm, stream);
     ZKX_CFAR_CASE(2, 2, 8, 8)
     ZKX_CFAR_CASE(1, 1, 4, 4)
     ZKX_CFAR_CASE(2, 2, 4, 4)
@@ -831,6 +892,30 @@ int launch_ca_cfar_compat(const float* x, int rank, int rows, int columns, int g
         x, cum, rank, rows, columns, gr, gc, rr, rc, alpha, nref, threshold, detections);
     ZKX_LAUNCHED("compat_threshold_kernel");
     return ZKX_SUCCESS;
+}
+
+bool wl_cfar_geometry(int gr, int gc, int rr, int rc, uint32_t* box_w, uint32_t* box_h)
+{
+#define ZKX_CFAR_CASE(A, B, C, D) \
+    if (gr == A && gc == B && rr == C && rc == D) { cfar_box<A, B, C, D>(box_w, box_h); return true; }
+    ZKX_CFAR_CASE(2, 2, 8, 8)
+    ZKX_CFAR_CASE(1, 1, 4, 4)
+    ZKX_CFAR_CASE(2, 2, 4, 4)
+    ZKX_CFAR_CASE(1, 1, 2, 2)
+#undef ZKX_CFAR_CASE
+    return false;
+}
+
+int launch_cfar_worklist(const WlCfarParams& p, int ctas, int gr, int gc, int rr, int rc, cudaStream_t stream)
+{
+#define ZKX_CFAR_CASE(A, B, C, D) \
+    if (gr == A && gc == B && rr == C && rc == D) return cfar_worklist_impl<A, B, C, D>(p, ctas, stream);
+    ZKX_CFAR_CASE(2, 2, 8, 8)
+    ZKX_CFAR_CASE(1, 1, 4, 4)
+    ZKX_CFAR_CASE(2, 2, 4, 4)
+    ZKX_CFAR_CASE(1, 1, 2, 2)
+#undef ZKX_CFAR_CASE
+    return fail(ZKX_UNSUPPORTED_OPERATION, "cfar work list: window geometry without a tiled kernel");
 }
 
 }  // namespace zkx

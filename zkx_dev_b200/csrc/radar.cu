@@ -18,6 +18,7 @@
 #include "tma.cuh"
 #include "window.cuh"
 #include "zkx_internal.h"
+#include "worklist.h"
 
 namespace zkx {
 namespace {
@@ -77,48 +78,69 @@ replica_spectrum_kernel(const float2* __restrict__ h, int length, int normalize,
 
 // Range compression lengths with a persistent kernel (N >= 4096) and a three-pass plan
 // read the second-pass twiddles from a shared table in both compression kernels.
-template <int N>
+template <int N, int E = elems_for(N)>
 constexpr bool compression_mid_table()
 {
-    return N >= 4096 && mid_table_elems<FftPlan<N, elems_for(N)>>() > 0;
+    return N >= 4096 && mid_table_elems<FftPlan<N, E>>() > 0;
 }
 
-// G pulses per CTA; each pulse: load (zero-pad/truncate to N), forward FFT, multiply
-// by the replica spectrum, inverse FFT, store.  The cube crosses HBM once each way.
-template <int N, int G, class Src>
-__global__ void __launch_bounds__(G * FftPlan<N, elems_for(N)>::T)
-pulse_compression_kernel(const Src src, int pulses, int samples,
-                         const float2* __restrict__ spectrum, float2* __restrict__ y,
-                         const float2* __restrict__ tw)
+// G transforms per CTA, thread group g = threadIdx.x / T: load row xr (zero-pad/truncate
+// to N; null: an idle group), forward FFT, multiply by the replica spectrum, inverse FFT,
+// store to yr (null: nothing stored).  Shared by the one-launch-per-pulse-group kernel and
+// the work-list kernel, so both round identically.
+template <int N, int E, int G>
+__device__ __forceinline__ void compress_rows(const float2* __restrict__ xr, int samples,
+                                              const float2* __restrict__ spectrum, float2* __restrict__ yr,
+                                              const float2* __restrict__ tw, float2* sm)
 {
-    using PL = FftPlan<N, elems_for(N)>;
-    extern __shared__ float2 sm[];
+    using PL = FftPlan<N, E>;
     const int g = threadIdx.x / PL::T;
     const int t = threadIdx.x - g * PL::T;
-    const int pulse = blockIdx.x * G + g;
-    const bool active = pulse < pulses;
     float2* smg = sm + g * PL::smem_elems();
     // lengths that also have the persistent kernel take its second-pass twiddle table,
     // so both kernels round identically and the tuning choice never changes a result
-    float2* mid = compression_mid_table<N>() ? sm + G * PL::smem_elems() : nullptr;
+    float2* mid = compression_mid_table<N, E>() ? sm + G * PL::smem_elems() : nullptr;
     if (mid) fill_mid_table<PL>(mid, threadIdx.x, G * PL::T, tw);
-    const float2* xr = active ? src.row(pulse) : nullptr;
     float2 v[PL::E];
 #pragma unroll
     for (int r = 0; r < PL::E; ++r) {
         const int e = t + PL::T * r;
-        v[r] = (active && e < samples) ? __ldcs(&xr[e]) : make_float2(0.f, 0.f);
+        v[r] = (xr != nullptr && e < samples) ? __ldcs(&xr[e]) : make_float2(0.f, 0.f);
     }
     fft_block<PL, -1, 1>(v, smg, t, tw, mid);
 #pragma unroll
     for (int r = 0; r < PL::E; ++r) v[r] = cmul(v[r], __ldg(&spectrum[t + PL::T * r]));
     if constexpr (PL::PASSES > 1) __syncthreads();
     fft_block<PL, 1, 1>(v, smg, t, tw, mid);
-    if (active) {
-        float2* yr = y + (size_t)pulse * N;
+    if (yr != nullptr) {
 #pragma unroll
         for (int r = 0; r < PL::E; ++r) yr[t + PL::T * r] = v[r];  // stays in L2 for the next stage
     }
+}
+
+// Shared memory of compress_rows<N, E, G>.
+template <int N, int E, int G>
+constexpr size_t compress_rows_smem()
+{
+    using PL = FftPlan<N, E>;
+    return ((size_t)G * PL::smem_elems() + (compression_mid_table<N, E>() ? mid_table_elems<PL>() : 0)) *
+           sizeof(float2);
+}
+
+// G pulses per CTA; each pulse: load (zero-pad/truncate to N), forward FFT, multiply
+// by the replica spectrum, inverse FFT, store.  The cube crosses HBM once each way.
+template <int N, int E, int G, class Src>
+__global__ void __launch_bounds__(G * FftPlan<N, E>::T)
+pulse_compression_kernel(const Src src, int pulses, int samples,
+                         const float2* __restrict__ spectrum, float2* __restrict__ y,
+                         const float2* __restrict__ tw)
+{
+    using PL = FftPlan<N, E>;
+    extern __shared__ float2 sm[];
+    const int pulse = blockIdx.x * G + (int)(threadIdx.x / PL::T);
+    const bool active = pulse < pulses;
+    compress_rows<N, E, G>(active ? src.row(pulse) : nullptr, samples, spectrum,
+                        active ? y + (size_t)pulse * N : nullptr, tw, sm);
 }
 
 // Persistent variant for long pulses (one 512-thread CTA per SM holds a whole
@@ -128,13 +150,13 @@ pulse_compression_kernel(const Src src, int pulses, int samples,
 // copies of the CTA's next pulse into that buffer, so the load streams in while the
 // current results are being stored.  Pulses are read from the staged copy
 // (unpadded, element e at sm[e]), zero beyond `samples`.
-template <int N, class Src>
-__global__ void __launch_bounds__(FftPlan<N, elems_for(N)>::T)
+template <int N, int E, class Src>
+__global__ void __launch_bounds__(FftPlan<N, E>::T)
 pulse_compression_persistent_kernel(const Src src, int pulses, int samples,
                                     const float2* __restrict__ spectrum, float2* __restrict__ y,
                                     const float2* __restrict__ tw, int* err)
 {
-    using PL = FftPlan<N, elems_for(N)>;
+    using PL = FftPlan<N, E>;
     extern __shared__ __align__(128) float2 sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + PL::smem_elems());
     // second-pass twiddles, the same for every pulse the CTA transforms
@@ -435,37 +457,42 @@ pulse_doppler_kernel(const float2* __restrict__ x, int pulses, int samples,
     }
 }
 
-// TMA-fed variant (16 columns): one thread issues the tile's 2-D bulk copies
-// (boxes of 16 columns x up to 256 pulses, pulses beyond the input zero-filled by the
-// copy engine) and the CTA waits on an mbarrier.  Row-strided tiles reach much higher
-// bandwidth this way than with per-thread loads, whose throughput is bounded by the
-// requests a thread can keep in flight.  The tile buffer doubles as the exchange
-// buffer once every thread has read its values.
+// TMA-fed Doppler tile: one thread issues the tile's 2-D bulk copies (boxes of C
+// columns x up to 256 pulses, pulses beyond the input zero-filled by the copy engine)
+// and the CTA waits on an mbarrier.  Row-strided tiles reach much higher bandwidth this
+// way than with per-thread loads, whose throughput is bounded by the requests a thread
+// can keep in flight.  The tile buffer doubles as the exchange buffer once every thread
+// has read its values.  Tile = columns col0 .. col0+C-1 of CPI `cpi`, whose pulses are
+// rows cpi*pulses .. of the map; out and power point at this CPI's planes.  Returns
+// false (error word set) if the copy did not complete.  Shared by the per-shape kernel
+// and the work-list kernel.
 template <int N, int C>
-__global__ void __launch_bounds__(C * FftPlan<N, elems_for(N)>::T)
-pulse_doppler_tma_kernel(const __grid_constant__ CUtensorMap tmap, int pulses, int samples,
-                         const float* __restrict__ window, float2* __restrict__ out,
-                         float* __restrict__ power, const float2* __restrict__ tw, int* err)
+constexpr int doppler_tile_span()
+{
+    using PL = FftPlan<N, elems_for(N)>;
+    // the exchange of a narrower tile is padded and can outgrow the landed tile
+    return C < 16 && C * PL::smem_elems(true) > N * C ? C * PL::smem_elems(true) : N * C;
+}
+
+template <int N, int C>
+__device__ __forceinline__ bool doppler_tma_tile(const CUtensorMap* tmap, int pulses, int samples, int cpi,
+                                                 int col0, const float* __restrict__ window,
+                                                 float2* __restrict__ out, float* __restrict__ power,
+                                                 const float2* __restrict__ tw, int* err, float2* sm)
 {
     using PL = FftPlan<N, elems_for(N)>;
     constexpr int BOXH = N < 256 ? N : 256;
-    extern __shared__ __align__(128) float2 sm[];
-    // the exchange of a narrower tile is padded and can outgrow the landed tile
-    constexpr int SPAN = C < 16 && C * PL::smem_elems(true) > N * C ? C * PL::smem_elems(true) : N * C;
+    constexpr int SPAN = doppler_tile_span<N, C>();
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + SPAN);
     const int c = threadIdx.x % C;
     const int t = threadIdx.x / C;
-    const int col0 = blockIdx.x * C;
-    const int cpi = blockIdx.y;  // CPI of a stacked batch: rows cpi*pulses .. +pulses-1
-    if (out) out += (size_t)cpi * N * samples;
-    if (power) power += (size_t)cpi * N * samples;
     if (threadIdx.x == 0) mbar_init(bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(bar, (uint32_t)(N * C * sizeof(float2)));
 #pragma unroll
         for (int b = 0; b < N / BOXH; ++b)
-            tma_load_2d(sm + b * BOXH * C, &tmap, 2 * col0, cpi * pulses + b * BOXH, bar);
+            tma_load_2d(sm + b * BOXH * C, tmap, 2 * col0, cpi * pulses + b * BOXH, bar);
     }
     // the window weights and the first pass's twiddle bases arrive while the tile is
     // in flight
@@ -480,7 +507,7 @@ pulse_doppler_tma_kernel(const __grid_constant__ CUtensorMap tmap, int pulses, i
     const bool ok = mbar_wait_bounded(bar, 0);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
-        return;
+        return false;
     }
     const int col = col0 + c;
     const bool active = col < samples;
@@ -506,6 +533,21 @@ pulse_doppler_tma_kernel(const __grid_constant__ CUtensorMap tmap, int pulses, i
             if (power) power[o] = fmaf(v[r].x, v[r].x, v[r].y * v[r].y);  // read next by CFAR
         }
     }
+    return true;
+}
+
+// Per-shape Doppler: CTA (x, y) = column tile x of CPI y of a stacked batch.
+template <int N, int C>
+__global__ void __launch_bounds__(C * FftPlan<N, elems_for(N)>::T)
+pulse_doppler_tma_kernel(const __grid_constant__ CUtensorMap tmap, int pulses, int samples,
+                         const float* __restrict__ window, float2* __restrict__ out,
+                         float* __restrict__ power, const float2* __restrict__ tw, int* err)
+{
+    extern __shared__ __align__(128) float2 sm[];
+    const int cpi = blockIdx.y;
+    doppler_tma_tile<N, C>(&tmap, pulses, samples, cpi, blockIdx.x * C, window,
+                           out ? out + (size_t)cpi * N * samples : nullptr,
+                           power ? power + (size_t)cpi * N * samples : nullptr, tw, err, sm);
 }
 
 __global__ void doppler_window_kernel(int pulses, int kind, const float* explicit_window,
@@ -563,12 +605,57 @@ int default_variant_for(int pulses, int slots)
     return pulses >= 4 * slots ? ZKX_COMPRESSION_LOCAL : ZKX_COMPRESSION_PLAIN;
 }
 
+// The Stockham-ordered compression with E values per thread: the persistent bulk-copy
+// pipeline (variant ZKX_COMPRESSION_PERSISTENT, 16-byte aligned pulses, N >= 4096) or
+// the one-launch-per-pulse-group kernel; both round identically.  ctas_per_sm > 0 caps the
+// persistent kernel's CTAs per SM.
+template <int N, int E, class Src>
+int stockham_compression(const Src& x, bool aligned16, int pulses, int samples, const float2* spectrum,
+                         float2* y, int variant, int ctas_per_sm, cudaStream_t s)
+{
+    using PL = FftPlan<N, E>;
+    if constexpr (N >= 4096) {
+        if (aligned16 && variant != ZKX_COMPRESSION_PLAIN) {
+            int dev = 0, sms = 0;
+            ZKX_CUDA(cudaGetDevice(&dev));
+            ZKX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            const size_t smem = ((size_t)PL::smem_elems() + 2 + mid_table_elems<PL>() +
+                                 (size_t)PL::T * (ilog2(PL::E) | 1)) * sizeof(float2);
+            auto k = pulse_compression_persistent_kernel<N, E, Src>;
+            ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int per_sm = 0;
+            ZKX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, PL::T, smem));
+            per_sm = std::max(per_sm, 1);
+            if (ctas_per_sm > 0) per_sm = std::min(per_sm, ctas_per_sm);
+            const int grid = std::max(1, std::min(pulses, sms * per_sm));
+            k<<<grid, PL::T, smem, s>>>(x, pulses, samples, spectrum, y, twiddle_table(),
+                                        kernel_error_word());
+            ZKX_LAUNCHED("pulse_compression_persistent_kernel");
+            return ZKX_SUCCESS;
+        }
+    }
+    constexpr int G = PL::T >= 128 ? 1 : 128 / PL::T;   // >= 128 threads per CTA
+    const size_t smem = compress_rows_smem<N, E, G>();
+    auto k = pulse_compression_kernel<N, E, G, Src>;
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int blocks = (pulses + G - 1) / G;
+    k<<<blocks, G * PL::T, smem, s>>>(x, pulses, samples, spectrum, y, twiddle_table());
+    ZKX_LAUNCHED("pulse_compression_kernel");
+    return ZKX_SUCCESS;
+}
+
+// Values per thread of the Stockham compression kernels besides the table's (the radix
+// plan the autotuner may choose): 32 <-> 16 where the CTA stays within 32 .. 512 threads.
+constexpr int alt_compression_radix(int n)
+{
+    return n < 1024 || n > 8192 ? 0 : (elems_for(n) == 32 ? 16 : 32);
+}
+
 template <int N, class Src>
 int compression_impl(const Src& x, bool aligned16, int pulses, int samples, const float2* spectrum,
-                     float2* y, int variant, cudaStream_t s)
+                     float2* y, int variant, int radix, int ctas_per_sm, cudaStream_t s)
 {
     if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
-    using PL = FftPlan<N, elems_for(N)>;
     if constexpr (local_fft_for(N)) {
         if (variant == ZKX_COMPRESSION_DEFAULT) {
             int slots = 0;
@@ -579,6 +666,12 @@ int compression_impl(const Src& x, bool aligned16, int pulses, int samples, cons
             using LP = LocalPlan<N>;
             int slots = 0;
             ZKX_TRY(local_compression_slots<N>(&slots));
+            if (ctas_per_sm > 0) {
+                int dev = 0, sms = 0;
+                ZKX_CUDA(cudaGetDevice(&dev));
+                ZKX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+                slots = std::min(slots, sms * ctas_per_sm);
+            }
             const size_t smem = local_compression_smem<N>();
             const bool pairs = (reinterpret_cast<uintptr_t>(y) & 15) == 0;
             auto k = pairs ? pulse_compression_local_kernel<N, Src, true> : pulse_compression_local_kernel<N, Src, false>;
@@ -589,35 +682,14 @@ int compression_impl(const Src& x, bool aligned16, int pulses, int samples, cons
             return ZKX_SUCCESS;
         }
     }
-    if constexpr (N >= 4096) {
-        // persistent bulk-copy pipeline: 16-byte aligned pulses (even length, aligned bases);
-        // variant ZKX_COMPRESSION_PLAIN keeps the one-launch-per-pulse-group kernel
-        if (aligned16 && variant != ZKX_COMPRESSION_PLAIN) {
-            int dev = 0, sms = 0;
-            ZKX_CUDA(cudaGetDevice(&dev));
-            ZKX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            const size_t smem = ((size_t)PL::smem_elems() + 2 + mid_table_elems<PL>() +
-                                 (size_t)PL::T * (ilog2(PL::E) | 1)) * sizeof(float2);
-            auto k = pulse_compression_persistent_kernel<N, Src>;
-            ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            int per_sm = 0;
-            ZKX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, PL::T, smem));
-            const int grid = std::max(1, std::min(pulses, sms * std::max(per_sm, 1)));
-            k<<<grid, PL::T, smem, s>>>(x, pulses, samples, spectrum, y, twiddle_table(),
-                                        kernel_error_word());
-            ZKX_LAUNCHED("pulse_compression_persistent_kernel");
-            return ZKX_SUCCESS;
-        }
+    constexpr int ALT = alt_compression_radix(N);
+    if constexpr (ALT != 0) {
+        if (radix == ALT)
+            return stockham_compression<N, ALT, Src>(x, aligned16, pulses, samples, spectrum, y, variant,
+                                                     ctas_per_sm, s);
     }
-    constexpr int G = rows_per_cta(N);
-    const size_t smem = ((size_t)G * PL::smem_elems() +
-                         (compression_mid_table<N>() ? mid_table_elems<PL>() : 0)) * sizeof(float2);
-    auto k = pulse_compression_kernel<N, G, Src>;
-    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int blocks = (pulses + G - 1) / G;
-    k<<<blocks, G * PL::T, smem, s>>>(x, pulses, samples, spectrum, y, twiddle_table());
-    ZKX_LAUNCHED("pulse_compression_kernel");
-    return ZKX_SUCCESS;
+    return stockham_compression<N, elems_for(N), Src>(x, aligned16, pulses, samples, spectrum, y, variant,
+                                                      ctas_per_sm, s);
 }
 
 template <int N, int CT>
@@ -625,8 +697,7 @@ int doppler_tma(const CUtensorMap& map, int pulses, int samples, const float* wi
                 float* power, int batch, cudaStream_t s)
 {
     using PL = FftPlan<N, elems_for(N)>;
-    constexpr int SPAN = CT < 16 && CT * PL::smem_elems(true) > N * CT ? CT * PL::smem_elems(true) : N * CT;
-    const size_t smem = (size_t)SPAN * sizeof(float2) + 16;
+    const size_t smem = (size_t)doppler_tile_span<N, CT>() * sizeof(float2) + 16;
     auto k = pulse_doppler_tma_kernel<N, CT>;
     ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const dim3 tiles((samples + CT - 1) / CT, batch);
@@ -692,6 +763,114 @@ int fft_rows_impl(const float2* x, int rows, int inverse, float2* y, cudaStream_
     return ZKX_SUCCESS;
 }
 
+// ------------------------------------------------------------------ work list
+
+// Group of a work-list CTA: the last group whose first CTA is at or before blockIdx.x.
+template <class Params>
+__device__ __forceinline__ int wl_group(const Params& p)
+{
+    int g = 0;
+    while (g + 1 < p.groups && (int)blockIdx.x >= p.g[g + 1].entry0) ++g;
+    return g;
+}
+
+// CTA `local` of a compression group: 512 / T pulses of the group's flattened pulse list
+// (CPI q / pulses, pulse q % pulses), the same transform code as pulse_compression_kernel.
+template <int N>
+__device__ __forceinline__ void wl_compress(const WlCompressionGroup& G, int local, const float2* tw, float2* sm)
+{
+    using PL = FftPlan<N, elems_for(N)>;
+    constexpr int GR = kWlCompressionThreads / PL::T;
+    const int q = local * GR + (int)(threadIdx.x / PL::T);
+    const bool active = q < G.rows;
+    const float2* xr = active ? G.xs[q / G.pulses] + (size_t)(q % G.pulses) * G.samples : nullptr;
+    compress_rows<N, elems_for(N), GR>(xr, G.samples, G.spectrum, active ? G.y + (size_t)q * N : nullptr, tw, sm);
+}
+
+template <int N>
+constexpr size_t wl_compress_smem()
+{
+    return compress_rows_smem<N, elems_for(N), kWlCompressionThreads / FftPlan<N, elems_for(N)>::T>();
+}
+
+constexpr size_t wl_compression_smem()
+{
+    size_t m = 0;
+    const size_t s[] = {wl_compress_smem<64>(),   wl_compress_smem<128>(),  wl_compress_smem<256>(),
+                        wl_compress_smem<512>(),  wl_compress_smem<1024>(), wl_compress_smem<2048>(),
+                        wl_compress_smem<4096>(), wl_compress_smem<8192>(), wl_compress_smem<16384>()};
+    for (size_t v : s) m = v > m ? v : m;
+    return m;
+}
+
+// Range compression of every CPI of the work list, whatever its length: one CTA per
+// (group, 512 / T pulses) entry, the code path chosen by the group's length.
+__global__ void __launch_bounds__(kWlCompressionThreads)
+compression_worklist_kernel(const __grid_constant__ WlCompressionParams p, const float2* __restrict__ tw)
+{
+    extern __shared__ __align__(16) float2 sm[];
+    const WlCompressionGroup& G = p.g[wl_group(p)];
+    const int local = (int)blockIdx.x - G.entry0;
+    switch (G.nfft) {
+    case 64: wl_compress<64>(G, local, tw, sm); break;
+    case 128: wl_compress<128>(G, local, tw, sm); break;
+    case 256: wl_compress<256>(G, local, tw, sm); break;
+    case 512: wl_compress<512>(G, local, tw, sm); break;
+    case 1024: wl_compress<1024>(G, local, tw, sm); break;
+    case 2048: wl_compress<2048>(G, local, tw, sm); break;
+    case 4096: wl_compress<4096>(G, local, tw, sm); break;
+    case 8192: wl_compress<8192>(G, local, tw, sm); break;
+    case 16384: wl_compress<16384>(G, local, tw, sm); break;
+    default: break;
+    }
+}
+
+// CTA `local` of a Doppler group: column tile local % tiles_x of CPI local / tiles_x,
+// 256 / T columns, the same tile code as pulse_doppler_tma_kernel; power only.
+template <int N>
+__device__ __forceinline__ void wl_doppler(const WlDopplerGroup& G, int local, const float2* tw, int* err,
+                                           float2* sm)
+{
+    constexpr int C = kWlDopplerThreads / FftPlan<N, elems_for(N)>::T;
+    const int b = local / G.tiles_x;
+    const int tile = local - b * G.tiles_x;
+    doppler_tma_tile<N, C>(&G.map, G.pulses, G.nr, b, tile * C, G.window, nullptr,
+                           G.power + (size_t)b * N * G.nr, tw, err, sm);
+}
+
+template <int N>
+constexpr size_t wl_doppler_smem_for()
+{
+    return (size_t)doppler_tile_span<N, kWlDopplerThreads / FftPlan<N, elems_for(N)>::T>() * sizeof(float2) + 16;
+}
+
+constexpr size_t wl_doppler_smem()
+{
+    size_t m = 0;
+    const size_t s[] = {wl_doppler_smem_for<64>(), wl_doppler_smem_for<128>(), wl_doppler_smem_for<256>(),
+                        wl_doppler_smem_for<512>(), wl_doppler_smem_for<1024>()};
+    for (size_t v : s) m = v > m ? v : m;
+    return m;
+}
+
+// Slow-time transform + window + |.|^2 of every CPI of the work list: one CTA per
+// (group, CPI, column tile) entry, the code path chosen by the group's Doppler length.
+__global__ void __launch_bounds__(kWlDopplerThreads)
+doppler_worklist_kernel(const __grid_constant__ WlDopplerParams p, const float2* __restrict__ tw, int* err)
+{
+    extern __shared__ __align__(128) float2 sm[];
+    const WlDopplerGroup& G = p.g[wl_group(p)];
+    const int local = (int)blockIdx.x - G.entry0;
+    switch (G.nd) {
+    case 64: wl_doppler<64>(G, local, tw, err, sm); break;
+    case 128: wl_doppler<128>(G, local, tw, err, sm); break;
+    case 256: wl_doppler<256>(G, local, tw, err, sm); break;
+    case 512: wl_doppler<512>(G, local, tw, err, sm); break;
+    case 1024: wl_doppler<1024>(G, local, tw, err, sm); break;
+    default: break;
+    }
+}
+
 #define ZKX_DISPATCH_POW2(LOG, CALL)                                                    \
     switch (LOG) {                                                                      \
     case 0: return CALL(1);     case 1: return CALL(2);     case 2: return CALL(4);     \
@@ -727,14 +906,15 @@ int launch_pulse_compression(const float2* x, int pulses, int samples, int nfft,
 }
 
 int launch_pulse_compression_variant(const float2* x, int pulses, int samples, int nfft,
-                                     const float2* spectrum, float2* y, int variant, cudaStream_t stream)
+                                     const float2* spectrum, float2* y, int variant, cudaStream_t stream,
+                                     int radix, int ctas_per_sm)
 {
     const RowsContiguous src{x, samples};
     if (!is_pow2(nfft)) return launch_compression_any(src, pulses, samples, nfft, spectrum, y, stream);
     if (nfft > (1 << kMaxSmemFftLog))
         return launch_long_compression(src, pulses, samples, nfft, spectrum, y, variant, stream);
     const bool aligned16 = (samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0;
-#define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, variant, stream)
+#define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, variant, radix, ctas_per_sm, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
 #undef ZKX_CALL
 }
@@ -758,7 +938,7 @@ int resolve_compression_variant(int pulses, int nfft, int variant, int* resolved
 
 int launch_pulse_compression_table(const float2* const* cpis, int count, int pulses_per_cpi,
                                    int samples, int nfft, const float2* spectrum, float2* y,
-                                   int variant, cudaStream_t stream)
+                                   int variant, cudaStream_t stream, int radix, int ctas_per_sm)
 {
     if (count < 1 || count > kMaxRowTable)
         return fail(ZKX_INVALID_ARGUMENT, "pulse_compression: 1 to 64 CPIs per table launch");
@@ -774,7 +954,7 @@ int launch_pulse_compression_table(const float2* const* cpis, int count, int pul
     if (!is_pow2(nfft)) return launch_compression_any(src, pulses, samples, nfft, spectrum, y, stream);
     if (nfft > (1 << kMaxSmemFftLog))
         return launch_long_compression(src, pulses, samples, nfft, spectrum, y, variant, stream);
-#define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, variant, stream)
+#define ZKX_CALL(NN) compression_impl<NN>(src, aligned16, pulses, samples, spectrum, y, variant, radix, ctas_per_sm, stream)
     ZKX_DISPATCH_POW2(ilog2_host(nfft), ZKX_CALL)
 #undef ZKX_CALL
 }
@@ -805,6 +985,59 @@ int launch_doppler_window(int pulses, int window_kind, const float* explicit_win
                                                                     explicit_window, out);
     ZKX_LAUNCHED("doppler_window_kernel");
     return ZKX_SUCCESS;
+}
+
+bool wl_compression_length(int n)
+{
+    return is_pow2(n) && n >= 64 && n <= (1 << kMaxSmemFftLog);
+}
+
+int wl_compression_ctas(int n, int rows)
+{
+    const int per = kWlCompressionThreads / (n / elems_for(n));
+    return (rows + per - 1) / per;
+}
+
+int launch_compression_worklist(const WlCompressionParams& p, int ctas, cudaStream_t stream)
+{
+    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
+    constexpr size_t smem = wl_compression_smem();
+    auto k = compression_worklist_kernel;
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<ctas, kWlCompressionThreads, smem, stream>>>(p, twiddle_table());
+    ZKX_LAUNCHED("compression_worklist_kernel");
+    return ZKX_SUCCESS;
+}
+
+bool wl_doppler_length(int n)
+{
+    return is_pow2(n) && n >= 64 && n <= 1024;
+}
+
+int wl_doppler_columns(int n)
+{
+    return kWlDopplerThreads / (n / elems_for(n));
+}
+
+int wl_doppler_box_rows(int n)
+{
+    return n < 256 ? n : 256;
+}
+
+int launch_doppler_worklist(const WlDopplerParams& p, int ctas, cudaStream_t stream)
+{
+    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
+    constexpr size_t smem = wl_doppler_smem();
+    auto k = doppler_worklist_kernel;
+    ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<ctas, kWlDopplerThreads, smem, stream>>>(p, twiddle_table(), kernel_error_word());
+    ZKX_LAUNCHED("doppler_worklist_kernel");
+    return ZKX_SUCCESS;
+}
+
+int compression_alt_radix(int nfft)
+{
+    return is_pow2(nfft) ? alt_compression_radix(nfft) : 0;
 }
 
 }  // namespace zkx

@@ -80,9 +80,13 @@ int launch_pulse_compression_tc(const float2* x, int pulses, int samples, int nf
                                 const float2* spectrum, float2* y, int precision,
                                 cudaStream_t stream);
 // Compression kernel choice: the library's default, the one-launch-per-pulse-group kernel,
-// or the persistent bulk-copy pipeline (N >= 4096, 16-byte aligned pulses).
+// the persistent bulk-copy pipeline (N >= 4096, 16-byte aligned pulses) or the four-step
+// kernels.  radix: values per thread of the first two (0 = the plan table's; the other of
+// 16 / 32 at nfft 1024 .. 8192, which rounds differently); ctas_per_sm > 0 caps the
+// persistent and four-step kernels' CTAs per SM (results unchanged).
 int launch_pulse_compression_variant(const float2* x, int pulses, int samples, int nfft,
-                                     const float2* spectrum, float2* y, int variant, cudaStream_t stream);
+                                     const float2* spectrum, float2* y, int variant, cudaStream_t stream,
+                                     int radix = 0, int ctas_per_sm = 0);
 // columns: range columns per CTA of the bulk-copy Doppler kernel (8 or 16; 0 = by shape).
 int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft,
                          const float* window, float2* out, float* power, int batch, int columns,
@@ -110,7 +114,9 @@ int resolve_compression_variant(int pulses, int nfft, int variant, int* resolved
 // `variant` is a ZKX_COMPRESSION_* choice, as for launch_pulse_compression_variant.
 int launch_pulse_compression_table(const float2* const* cpis, int count, int pulses_per_cpi,
                                    int samples, int nfft, const float2* spectrum, float2* y,
-                                   int variant, cudaStream_t stream);
+                                   int variant, cudaStream_t stream, int radix = 0, int ctas_per_sm = 0);
+// The other radix plan the Stockham compression kernels have at nfft (0: none).
+int compression_alt_radix(int nfft);
 int launch_long_fft_rows(const float2* x, int rows, int n, int inverse, float2* y,
                          cudaStream_t stream);
 int launch_doppler_window(int pulses, int window_kind, const float* explicit_window, float* out,
@@ -120,7 +126,8 @@ int launch_doppler_window(int pulses, int window_kind, const float* explicit_win
 int launch_ca_cfar_accurate(const float* x, int rows, int columns, int guard_rows,
                             int guard_columns, int reference_rows, int reference_columns,
                             double alpha, int reference_count, float* threshold,
-                            uint8_t* detections, int batch, int tile, cudaStream_t stream);
+                            uint8_t* detections, int batch, int tile, cudaStream_t stream,
+                            int ctas_per_sm = 0);
 int launch_ca_cfar_compat(const float* x, int rank, int rows, int columns, int guard_rows,
                           int guard_columns, int reference_rows, int reference_columns,
                           float alpha, int reference_count, float* cumulative, float* threshold,
@@ -138,6 +145,18 @@ int launch_fir_fft(const float* b, int nb, const float* x, int lines, int n, con
 int rd_execute_batch_ws(zkx_rd_plan p, const void* x, int batch, void* compressed, void* rd,
                         float* power, float* threshold, uint8_t* detections, float* cumulative,
                         cudaStream_t stream, const void* const* table = nullptr);
+// Read-only view of a plan's resident state (capi.cu), for the work-list builder.
+struct RdPlanView {
+    zkx_rd_desc d;
+    int range_nfft, doppler_nfft;
+    const float2* spectrum;
+    const float* doppler_window;   // null without a window
+    float* cumulative;             // compat-mode integral image (null in accurate mode)
+    double alpha;
+    int nref;
+    zkx_rd_tuning tuning;
+};
+int rd_plan_view(zkx_rd_plan p, RdPlanView* v);
 // Transforms of any length (bluestein.cu): lengths that are not powers of two up to
 // kMaxBluesteinLength by the chirp-z identity on power-of-two FFTs; spectra in natural order.
 constexpr int kMaxBluesteinLength = 1 << 15;
