@@ -484,13 +484,15 @@ ZKX_API int zkx_rd_graph_destroy(zkx_rd_graph graph);
  * plan, allocates the compressed cubes and power planes of every CPI (grouped by plan,
  * library-owned) and device tables of the items' pointers, and builds the stage kernels'
  * parameter blocks; launch enqueues on `stream`
- *   range compression  one work-list kernel over every (CPI, 512-thread pulse group)
- *                      entry with a range nfft that is a power of two from 64 to 16384;
- *   Doppler + |.|^2    one work-list kernel over every (CPI, column tile) entry with a
+ *   range compression  work-list kernels over every (CPI, 256-thread pulse group) entry
+ *                      with a range nfft that is a power of two from 64 to 8192;
+ *   Doppler + |.|^2    work-list kernels over every (CPI, column tile) entry with a
  *                      Doppler nfft that is a power of two from 64 to 1024;
  *   CA-CFAR            one work-list kernel over every (CPI, 64 x 64 tile) entry of the
  *                      accurate mode with the tiled window geometry of the first such plan;
- * (at most 24 plans per launch: more plans take one launch per 24).  A plan whose stage
+ * compression and Doppler take one launch per resource class present (lengths with up to
+ * 16 values per thread, and with 32), each class its own registers and shared memory; at
+ * most 24 plans per launch (more plans take one launch per 24).  A plan whose stage
  * falls outside these (longer or non-power-of-two transforms, a tuning choice that rounds
  * differently from the work-list kernel, compat mode, another window geometry) runs that
  * stage with its own kernels, one launch per plan (per CPI for CFAR).  Every CPI's

@@ -62,7 +62,7 @@ def check_alone(items):
             assert torch.equal(out["power"], ref["power"]), i
 
 
-COVERED = [(64, 1024, 3, {}), (128, 4096, 2, {}), (256, 2048, 2, {}), (64, 16384, 2, {}),
+COVERED = [(64, 1024, 3, {}), (128, 4096, 2, {}), (256, 2048, 2, {}), (64, 4096, 2, {}),
            (64, 8192, 1, {}), (512, 512, 1, {}), (128, 256, 2, {}), (1024, 1024, 1, {}),
            (100, 2048, 3, {"doppler_nfft": 128})]   # Doppler zero padding: 100 pulses -> 128 bins
 
@@ -71,11 +71,12 @@ def test_worklist_equals_each_cpi_alone(z):
     items, _ = make_items(z, COVERED, 1)
     wl = z.WorkList(items)
     info = wl.info()
-    # every stage of every plan on the work-list kernels: three launches, plus the
-    # copies of the power planes asked for
+    # every stage of every plan on the work-list kernels: compression and Doppler one
+    # launch per resource class (up to 16 and 32 values per thread), CFAR one launch, plus
+    # the copies of the power planes asked for
     powers = sum("power" in o for _, _, o in items)
     assert info["groups"] == len(COVERED)
-    assert info["launches"] == 3 + powers
+    assert info["launches"] == 5 + powers
     wl.launch()
     torch.cuda.synchronize()
     check_alone(items)
@@ -88,6 +89,7 @@ def test_worklist_stages_on_the_plans_own_kernels(z):
     specs = [
         (64, 1024, 2, {}),
         (1024, 16384, 1, {}),                       # four-step compression by default
+        (64, 16384, 2, {}),                         # 16384 points: the plan's own compression
         (64, 32768, 2, {}),                         # cluster compression
         (100, 1000, 2, {}),                         # chirp-z range and Doppler lengths
         (2048, 1024, 1, {}),                        # Doppler length 2048

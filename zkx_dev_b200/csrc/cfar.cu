@@ -614,52 +614,90 @@ cfar_accurate_tma2_kernel(const __grid_constant__ CUtensorMap tmap, int rows, in
     }
 }
 
-// CA-CFAR of every map of a work list, whatever its shape: one CTA per (group, map, 64 x 64
-// tile) entry, computed exactly as by cfar_accurate_tma_kernel (whose thresholds the
-// persistent kernel also reproduces); each map writes its own threshold and detection
-// planes.
+// CA-CFAR of every map of a work list, whatever its shape: the persistent double-buffered
+// walk of cfar_accurate_stream_kernel over the (group, map, 64 x 64 tile) entries of all
+// groups, each tile computed exactly as by cfar_accurate_tma_kernel (so the thresholds
+// equal the per-shape kernels'), each map writing its own threshold and detection planes.
 template <int GR, int GC, int RR, int RC>
 __global__ void __launch_bounds__(kCfarThreads, 2)
-cfar_worklist_kernel(const __grid_constant__ WlCfarParams p, int* err)
+cfar_worklist_kernel(const __grid_constant__ WlCfarParams p, int tiles, int* err)
 {
     using G = CfarTmaGeom<GR, GC, RR, RC>;
+    using GS = CfarStreamGeom<GR, GC, RR, RC>;
     extern __shared__ __align__(128) float csm[];
-    float* P = csm;                           // [HR][BOXW]
-    float* SA = P + G::HR * G::BOXW;          // [TY][PITCH]
+    // halo buffer b at csm + b * STRIDE
+    float* SA = csm + 2 * GS::STRIDE;         // [TY][PITCH]
     float* SB = SA + kCfarTY * G::PITCH;      // [TY][PITCH]
-    uint64_t* bar = reinterpret_cast<uint64_t*>(SB + kCfarTY * G::PITCH);
-    int gi = 0;
-    while (gi + 1 < p.groups && (int)blockIdx.x >= p.g[gi + 1].entry0) ++gi;
-    const WlCfarGroup& W = p.g[gi];
-    const int local = (int)blockIdx.x - W.entry0;
-    const int tx = local % W.tiles_x, rest = local / W.tiles_x;
-    const int ty = rest % W.tiles_y, b = rest / W.tiles_y;
-    const int r0 = ty * kCfarTY, c0 = tx * kCfarTX;
-    if (threadIdx.x == 0) mbar_init(bar, 1);
-    __syncthreads();
+    uint64_t* full = reinterpret_cast<uint64_t*>(SB + kCfarTY * G::PITCH);
+    const int step = (int)gridDim.x;
+    // entry -> group, map, tile row, tile column
+    auto locate = [&](int tile, int& gi, int& b, int& ty, int& tx) {
+        gi = 0;
+        while (gi + 1 < p.groups && tile >= p.g[gi + 1].entry0) ++gi;
+        const WlCfarGroup& W = p.g[gi];
+        const int local = tile - W.entry0;
+        tx = local % W.tiles_x;
+        const int rest = local / W.tiles_x;
+        ty = rest % W.tiles_y;
+        b = rest / W.tiles_y;
+    };
+    auto issue = [&](int tile, int buf) {
+        int gi, b, ty, tx;
+        locate(tile, gi, b, ty, tx);
+        mbar_arrive_expect_tx(&full[buf], (uint32_t)(GS::HALO * sizeof(float)));
+        tma_load_2d(csm + buf * GS::STRIDE, &p.g[gi].map, tx * kCfarTX - G::MC - G::OFF,
+                    b * p.g[gi].rows + ty * kCfarTY - G::MR, &full[buf]);
+    };
     if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(bar, (uint32_t)(G::HR * G::BOXW * sizeof(float)));
-        tma_load_2d(P, &W.map, c0 - G::MC - G::OFF, b * W.rows + r0 - G::MR, bar);
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
     }
-    const bool ok = mbar_wait_bounded(bar, 0);
-    if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) atomicCAS(err, 0, (int)kKernelTmaTimeout);
-        return;
-    }
-    full_tile_vertical<GR, GC, RR, RC>(P, SA, SB);
     __syncthreads();
-    full_tile_horizontal<GR, GC, RR, RC>(P, SA, SB, r0, c0, W.rows, W.cols, W.scale32, W.scale64, W.thr[b],
-                                         W.det[b]);
+    const int first = (int)blockIdx.x;
+    if (threadIdx.x == 0) {
+        if (first < tiles) issue(first, 0);
+        if (first + step < tiles) issue(first + step, 1);
+    }
+    int k = 0;
+    for (int tile = first; tile < tiles; tile += step, ++k) {
+        const int buf = k & 1;
+        const bool ok = mbar_wait_bounded(&full[buf], (uint32_t)((k >> 1) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                atomicCAS(err, 0, (int)kKernelTmaTimeout);
+                // the copy that timed out and the one into the other buffer may still be in
+                // flight: wait for them (bounded) before the shared memory is released
+                mbar_wait_bounded(&full[buf], (uint32_t)((k >> 1) & 1));
+                if (tile + step < tiles) mbar_wait_bounded(&full[buf ^ 1], (uint32_t)(((k + 1) >> 1) & 1));
+            }
+            return;
+        }
+        int gi, b, ty, tx;
+        locate(tile, gi, b, ty, tx);
+        const WlCfarGroup& W = p.g[gi];
+        const float* P = csm + buf * GS::STRIDE;
+        full_tile_vertical<GR, GC, RR, RC>(P, SA, SB);
+        __syncthreads();
+        full_tile_horizontal<GR, GC, RR, RC>(P, SA, SB, ty * kCfarTY, tx * kCfarTX, W.rows, W.cols, W.scale32,
+                                             W.scale64, W.thr[b], W.det[b]);
+        __syncthreads();   // halo buffer buf, SA and SB are free
+        if (threadIdx.x == 0 && tile + 2 * step < tiles) issue(tile + 2 * step, buf);
+    }
 }
 
 template <int GR, int GC, int RR, int RC>
-int cfar_worklist_impl(const WlCfarParams& p, int ctas, cudaStream_t s)
+int cfar_worklist_impl(const WlCfarParams& p, int tiles, cudaStream_t s)
 {
-    using G = CfarTmaGeom<GR, GC, RR, RC>;
-    const size_t smem = G::smem_bytes();
+    using GS = CfarStreamGeom<GR, GC, RR, RC>;
+    const size_t smem = GS::smem_bytes();
     auto k = cfar_worklist_kernel<GR, GC, RR, RC>;
     ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<ctas, kCfarThreads, smem, s>>>(p, kernel_error_word());
+    int dev = 0, sms = 0, per_sm = 0;
+    ZKX_CUDA(cudaGetDevice(&dev));
+    ZKX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    ZKX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kCfarThreads, smem));
+    const int ctas = std::max(1, std::min(tiles, sms * std::max(per_sm, 1)));
+    k<<<ctas, kCfarThreads, smem, s>>>(p, tiles, kernel_error_word());
     ZKX_LAUNCHED("cfar_worklist_kernel");
     return ZKX_SUCCESS;
 }
@@ -906,10 +944,10 @@ bool wl_cfar_geometry(int gr, int gc, int rr, int rc, uint32_t* box_w, uint32_t*
     return false;
 }
 
-int launch_cfar_worklist(const WlCfarParams& p, int ctas, int gr, int gc, int rr, int rc, cudaStream_t stream)
+int launch_cfar_worklist(const WlCfarParams& p, int tiles, int gr, int gc, int rr, int rc, cudaStream_t stream)
 {
 #define ZKX_CFAR_CASE(A, B, C, D) \
-    if (gr == A && gc == B && rr == C && rc == D) return cfar_worklist_impl<A, B, C, D>(p, ctas, stream);
+    if (gr == A && gc == B && rr == C && rc == D) return cfar_worklist_impl<A, B, C, D>(p, tiles, stream);
     ZKX_CFAR_CASE(2, 2, 8, 8)
     ZKX_CFAR_CASE(1, 1, 4, 4)
     ZKX_CFAR_CASE(2, 2, 4, 4)

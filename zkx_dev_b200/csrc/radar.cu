@@ -774,7 +774,12 @@ __device__ __forceinline__ int wl_group(const Params& p)
     return g;
 }
 
-// CTA `local` of a compression group: 512 / T pulses of the group's flattened pulse list
+// Work-list resource classes: lengths with up to 16 values per thread (class 0) and with
+// 32 (class 1) run in separate launches, so each kernel's registers and shared memory fit
+// its own lengths instead of the largest.
+constexpr int wl_class(int n) { return elems_for(n) == 32 ? 1 : 0; }
+
+// CTA `local` of a compression group: 256 / T pulses of the group's flattened pulse list
 // (CPI q / pulses, pulse q % pulses), the same transform code as pulse_compression_kernel.
 template <int N>
 __device__ __forceinline__ void wl_compress(const WlCompressionGroup& G, int local, const float2* tw, float2* sm)
@@ -787,24 +792,33 @@ __device__ __forceinline__ void wl_compress(const WlCompressionGroup& G, int loc
     compress_rows<N, elems_for(N), GR>(xr, G.samples, G.spectrum, active ? G.y + (size_t)q * N : nullptr, tw, sm);
 }
 
-template <int N>
+template <int N, int CLASS>
 constexpr size_t wl_compress_smem()
 {
-    return compress_rows_smem<N, elems_for(N), kWlCompressionThreads / FftPlan<N, elems_for(N)>::T>();
+    if constexpr (wl_class(N) != CLASS) return 0;
+    else return compress_rows_smem<N, elems_for(N), kWlCompressionThreads / FftPlan<N, elems_for(N)>::T>();
 }
 
+template <int CLASS>
 constexpr size_t wl_compression_smem()
 {
     size_t m = 0;
-    const size_t s[] = {wl_compress_smem<64>(),   wl_compress_smem<128>(),  wl_compress_smem<256>(),
-                        wl_compress_smem<512>(),  wl_compress_smem<1024>(), wl_compress_smem<2048>(),
-                        wl_compress_smem<4096>(), wl_compress_smem<8192>(), wl_compress_smem<16384>()};
+    const size_t s[] = {wl_compress_smem<64, CLASS>(),   wl_compress_smem<128, CLASS>(),
+                        wl_compress_smem<256, CLASS>(),  wl_compress_smem<512, CLASS>(),
+                        wl_compress_smem<1024, CLASS>(), wl_compress_smem<2048, CLASS>(),
+                        wl_compress_smem<4096, CLASS>(), wl_compress_smem<8192, CLASS>()};
     for (size_t v : s) m = v > m ? v : m;
     return m;
 }
 
-// Range compression of every CPI of the work list, whatever its length: one CTA per
-// (group, 512 / T pulses) entry, the code path chosen by the group's length.
+#define ZKX_WL_CASE(NN, CALL)                               \
+    case NN:                                                \
+        if constexpr (wl_class(NN) == CLASS) CALL;          \
+        break;
+
+// Range compression of every CPI of the work list with a length of this class: one CTA
+// per (group, 256 / T pulses) entry, the code path chosen by the group's length.
+template <int CLASS>
 __global__ void __launch_bounds__(kWlCompressionThreads)
 compression_worklist_kernel(const __grid_constant__ WlCompressionParams p, const float2* __restrict__ tw)
 {
@@ -812,15 +826,14 @@ compression_worklist_kernel(const __grid_constant__ WlCompressionParams p, const
     const WlCompressionGroup& G = p.g[wl_group(p)];
     const int local = (int)blockIdx.x - G.entry0;
     switch (G.nfft) {
-    case 64: wl_compress<64>(G, local, tw, sm); break;
-    case 128: wl_compress<128>(G, local, tw, sm); break;
-    case 256: wl_compress<256>(G, local, tw, sm); break;
-    case 512: wl_compress<512>(G, local, tw, sm); break;
-    case 1024: wl_compress<1024>(G, local, tw, sm); break;
-    case 2048: wl_compress<2048>(G, local, tw, sm); break;
-    case 4096: wl_compress<4096>(G, local, tw, sm); break;
-    case 8192: wl_compress<8192>(G, local, tw, sm); break;
-    case 16384: wl_compress<16384>(G, local, tw, sm); break;
+    ZKX_WL_CASE(64, (wl_compress<64>(G, local, tw, sm)))
+    ZKX_WL_CASE(128, (wl_compress<128>(G, local, tw, sm)))
+    ZKX_WL_CASE(256, (wl_compress<256>(G, local, tw, sm)))
+    ZKX_WL_CASE(512, (wl_compress<512>(G, local, tw, sm)))
+    ZKX_WL_CASE(1024, (wl_compress<1024>(G, local, tw, sm)))
+    ZKX_WL_CASE(2048, (wl_compress<2048>(G, local, tw, sm)))
+    ZKX_WL_CASE(4096, (wl_compress<4096>(G, local, tw, sm)))
+    ZKX_WL_CASE(8192, (wl_compress<8192>(G, local, tw, sm)))
     default: break;
     }
 }
@@ -838,23 +851,27 @@ __device__ __forceinline__ void wl_doppler(const WlDopplerGroup& G, int local, c
                            G.power + (size_t)b * N * G.nr, tw, err, sm);
 }
 
-template <int N>
+template <int N, int CLASS>
 constexpr size_t wl_doppler_smem_for()
 {
-    return (size_t)doppler_tile_span<N, kWlDopplerThreads / FftPlan<N, elems_for(N)>::T>() * sizeof(float2) + 16;
+    if constexpr (wl_class(N) != CLASS) return 0;
+    else return (size_t)doppler_tile_span<N, kWlDopplerThreads / FftPlan<N, elems_for(N)>::T>() * sizeof(float2) + 16;
 }
 
+template <int CLASS>
 constexpr size_t wl_doppler_smem()
 {
     size_t m = 0;
-    const size_t s[] = {wl_doppler_smem_for<64>(), wl_doppler_smem_for<128>(), wl_doppler_smem_for<256>(),
-                        wl_doppler_smem_for<512>(), wl_doppler_smem_for<1024>()};
+    const size_t s[] = {wl_doppler_smem_for<64, CLASS>(), wl_doppler_smem_for<128, CLASS>(),
+                        wl_doppler_smem_for<256, CLASS>(), wl_doppler_smem_for<512, CLASS>(),
+                        wl_doppler_smem_for<1024, CLASS>()};
     for (size_t v : s) m = v > m ? v : m;
     return m;
 }
 
-// Slow-time transform + window + |.|^2 of every CPI of the work list: one CTA per
-// (group, CPI, column tile) entry, the code path chosen by the group's Doppler length.
+// Slow-time transform + window + |.|^2 of every CPI of the work list with a Doppler length
+// of this class: one CTA per (group, CPI, column tile) entry.
+template <int CLASS>
 __global__ void __launch_bounds__(kWlDopplerThreads)
 doppler_worklist_kernel(const __grid_constant__ WlDopplerParams p, const float2* __restrict__ tw, int* err)
 {
@@ -862,14 +879,15 @@ doppler_worklist_kernel(const __grid_constant__ WlDopplerParams p, const float2*
     const WlDopplerGroup& G = p.g[wl_group(p)];
     const int local = (int)blockIdx.x - G.entry0;
     switch (G.nd) {
-    case 64: wl_doppler<64>(G, local, tw, err, sm); break;
-    case 128: wl_doppler<128>(G, local, tw, err, sm); break;
-    case 256: wl_doppler<256>(G, local, tw, err, sm); break;
-    case 512: wl_doppler<512>(G, local, tw, err, sm); break;
-    case 1024: wl_doppler<1024>(G, local, tw, err, sm); break;
+    ZKX_WL_CASE(64, (wl_doppler<64>(G, local, tw, err, sm)))
+    ZKX_WL_CASE(128, (wl_doppler<128>(G, local, tw, err, sm)))
+    ZKX_WL_CASE(256, (wl_doppler<256>(G, local, tw, err, sm)))
+    ZKX_WL_CASE(512, (wl_doppler<512>(G, local, tw, err, sm)))
+    ZKX_WL_CASE(1024, (wl_doppler<1024>(G, local, tw, err, sm)))
     default: break;
     }
 }
+#undef ZKX_WL_CASE
 
 #define ZKX_DISPATCH_POW2(LOG, CALL)                                                    \
     switch (LOG) {                                                                      \
@@ -989,7 +1007,12 @@ int launch_doppler_window(int pulses, int window_kind, const float* explicit_win
 
 bool wl_compression_length(int n)
 {
-    return is_pow2(n) && n >= 64 && n <= (1 << kMaxSmemFftLog);
+    return is_pow2(n) && n >= 64 && n <= 8192;
+}
+
+int wl_length_class(int n)
+{
+    return wl_class(n);
 }
 
 int wl_compression_ctas(int n, int rows)
@@ -998,15 +1021,21 @@ int wl_compression_ctas(int n, int rows)
     return (rows + per - 1) / per;
 }
 
-int launch_compression_worklist(const WlCompressionParams& p, int ctas, cudaStream_t stream)
+template <int CLASS>
+int compression_worklist_launch(const WlCompressionParams& p, int ctas, cudaStream_t stream)
 {
-    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
-    constexpr size_t smem = wl_compression_smem();
-    auto k = compression_worklist_kernel;
+    constexpr size_t smem = wl_compression_smem<CLASS>();
+    auto k = compression_worklist_kernel<CLASS>;
     ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<ctas, kWlCompressionThreads, smem, stream>>>(p, twiddle_table());
     ZKX_LAUNCHED("compression_worklist_kernel");
     return ZKX_SUCCESS;
+}
+
+int launch_compression_worklist(const WlCompressionParams& p, int ctas, int cls, cudaStream_t stream)
+{
+    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
+    return cls == 0 ? compression_worklist_launch<0>(p, ctas, stream) : compression_worklist_launch<1>(p, ctas, stream);
 }
 
 bool wl_doppler_length(int n)
@@ -1024,15 +1053,21 @@ int wl_doppler_box_rows(int n)
     return n < 256 ? n : 256;
 }
 
-int launch_doppler_worklist(const WlDopplerParams& p, int ctas, cudaStream_t stream)
+template <int CLASS>
+int doppler_worklist_launch(const WlDopplerParams& p, int ctas, cudaStream_t stream)
 {
-    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
-    constexpr size_t smem = wl_doppler_smem();
-    auto k = doppler_worklist_kernel;
+    constexpr size_t smem = wl_doppler_smem<CLASS>();
+    auto k = doppler_worklist_kernel<CLASS>;
     ZKX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<ctas, kWlDopplerThreads, smem, stream>>>(p, twiddle_table(), kernel_error_word());
     ZKX_LAUNCHED("doppler_worklist_kernel");
     return ZKX_SUCCESS;
+}
+
+int launch_doppler_worklist(const WlDopplerParams& p, int ctas, int cls, cudaStream_t stream)
+{
+    if (!twiddle_table()) return fail(ZKX_INTERNAL_ERROR, "twiddle table not initialised on this device");
+    return cls == 0 ? doppler_worklist_launch<0>(p, ctas, stream) : doppler_worklist_launch<1>(p, ctas, stream);
 }
 
 int compression_alt_radix(int nfft)

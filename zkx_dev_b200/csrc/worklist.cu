@@ -76,7 +76,7 @@ float* group_power(zkx_rd_worklist w, const WlGroup& g)
 
 // Which stages of a group the work-list kernels run.  The rules keep each CPI's bits
 // equal to the CPI executed alone with its plan:
-//   compression  a power-of-two range nfft of 64 .. 16384 whose plan runs the
+//   compression  a power-of-two range nfft of 64 .. 8192 whose plan runs the
 //                one-launch-per-pulse-group transform or the persistent Stockham kernel
 //                (the same bits) with the table's radix plan, not the four-step or cluster
 //                kernels;
@@ -125,11 +125,13 @@ int build_params(zkx_rd_worklist w)
     float* const* thr = reinterpret_cast<float* const*>(w->tables + count);
     uint8_t* const* det = reinterpret_cast<uint8_t* const*>(w->tables + 2 * count);
 
+    for (int cls : {0, 1})
     for (WlGroup& g : w->groups) {
-        if (!g.comp_wl) continue;
-        if (w->comp.empty() || w->comp.back().groups == kWlGroups) {
+        if (!g.comp_wl || wl_length_class(g.v.range_nfft) != cls) continue;
+        if (w->comp.empty() || w->comp.back().groups == kWlGroups || w->comp.back().cls != cls) {
             w->comp.emplace_back();
             std::memset(&w->comp.back(), 0, sizeof(WlCompressionParams));
+            w->comp.back().cls = cls;
             w->comp_ctas.push_back(0);
         }
         WlCompressionParams& p = w->comp.back();
@@ -145,8 +147,9 @@ int build_params(zkx_rd_worklist w)
         w->comp_ctas.back() += wl_compression_ctas(e.nfft, e.rows);
     }
 
+    for (int cls : {0, 1})
     for (WlGroup& g : w->groups) {
-        if (!g.dop_wl) continue;
+        if (!g.dop_wl || wl_length_class(g.v.doppler_nfft) != cls) continue;
         const int nr = g.v.range_nfft, nd = g.v.doppler_nfft, P = g.v.d.num_pulses;
         const int C = wl_doppler_columns(nd);
         CUtensorMap map;
@@ -155,9 +158,10 @@ int build_params(zkx_rd_worklist w)
             g.dop_wl = false;  // the plan's own Doppler launch instead
             continue;
         }
-        if (w->dop.empty() || w->dop.back().groups == kWlGroups) {
+        if (w->dop.empty() || w->dop.back().groups == kWlGroups || w->dop.back().cls != cls) {
             w->dop.emplace_back();
             std::memset(&w->dop.back(), 0, sizeof(WlDopplerParams));
+            w->dop.back().cls = cls;
             w->dop_ctas.push_back(0);
         }
         WlDopplerParams& p = w->dop.back();
@@ -221,7 +225,8 @@ int build_params(zkx_rd_worklist w)
 int launch_list(zkx_rd_worklist w, cudaStream_t s)
 {
     // range compression
-    for (size_t i = 0; i < w->comp.size(); ++i) ZKX_TRY(launch_compression_worklist(w->comp[i], w->comp_ctas[i], s));
+    for (size_t i = 0; i < w->comp.size(); ++i)
+        ZKX_TRY(launch_compression_worklist(w->comp[i], w->comp_ctas[i], w->comp[i].cls, s));
     for (const WlGroup& g : w->groups) {
         if (g.comp_wl) continue;
         const zkx_rd_desc& d = g.v.d;
@@ -237,7 +242,8 @@ int launch_list(zkx_rd_worklist w, cudaStream_t s)
         }
     }
     // Doppler + |.|^2
-    for (size_t i = 0; i < w->dop.size(); ++i) ZKX_TRY(launch_doppler_worklist(w->dop[i], w->dop_ctas[i], s));
+    for (size_t i = 0; i < w->dop.size(); ++i)
+        ZKX_TRY(launch_doppler_worklist(w->dop[i], w->dop_ctas[i], w->dop[i].cls, s));
     for (const WlGroup& g : w->groups) {
         if (g.dop_wl) continue;
         ZKX_TRY(launch_pulse_doppler(group_compressed(w, g), g.v.d.num_pulses, g.v.range_nfft, g.v.doppler_nfft,

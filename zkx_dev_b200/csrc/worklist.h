@@ -1,7 +1,9 @@
 // Work-list execution of the range-Doppler chain over CPIs of mixed shapes: the parameter
-// blocks of the three stage kernels and their launchers.  Each stage is ONE launch over
-// every (CPI, tile) entry of up to kWlGroups shape groups (a group = the CPIs of one plan);
-// a CTA finds its group from the groups' first entries, then runs that group's code path
+// blocks of the three stage kernels and their launchers.  A stage is one launch over every
+// (CPI, tile) entry of up to kWlGroups shape groups (a group = the CPIs of one plan) per
+// resource class: compression and Doppler lengths with up to 16 values per thread (class
+// 0) and with 32 (class 1) run in separate launches, each kernel sized for its own lengths.
+// A CTA finds its group from the groups' first entries, then runs that group's code path
 // (a switch over the transform length inside the kernel).  The per-group constants, the
 // bulk-copy tensor maps included, travel in the kernel's parameter block.
 #pragma once
@@ -14,7 +16,7 @@
 namespace zkx {
 
 constexpr int kWlGroups = 24;               // shape groups per launch
-constexpr int kWlCompressionThreads = 512;  // compression CTA: 512 / T(nfft) pulses
+constexpr int kWlCompressionThreads = 256;  // compression CTA: 256 / T(nfft) pulses
 constexpr int kWlDopplerThreads = 256;      // Doppler CTA: 256 / T(nfft) range columns
 
 struct WlCompressionGroup {
@@ -28,6 +30,7 @@ struct WlCompressionGroup {
 struct WlCompressionParams {
     WlCompressionGroup g[kWlGroups];
     int groups;
+    int cls;                   // resource class of every group of the launch
 };
 
 struct WlDopplerGroup {
@@ -41,6 +44,7 @@ struct WlDopplerGroup {
 struct WlDopplerParams {
     WlDopplerGroup g[kWlGroups];
     int groups;
+    int cls;
 };
 
 struct WlCfarGroup {
@@ -58,21 +62,24 @@ struct WlCfarParams {
     int groups;
 };
 
-// Range lengths the work-list compression kernel runs (powers of two 64 .. 16384), its
-// CTAs for `rows` pulses of length n, and its launch.
+// Range lengths the work-list compression kernel runs (powers of two 64 .. 8192), the
+// resource class of a length (compression and Doppler), the CTAs for `rows` pulses of
+// length n, and the launch of one class.
 bool wl_compression_length(int n);
+int wl_length_class(int n);
 int wl_compression_ctas(int n, int rows);
-int launch_compression_worklist(const WlCompressionParams& p, int ctas, cudaStream_t stream);
+int launch_compression_worklist(const WlCompressionParams& p, int ctas, int cls, cudaStream_t stream);
 
 // Doppler lengths the work-list Doppler kernel runs (powers of two 64 .. 1024), its
 // columns per CTA and bulk-copy box height, and its launch.
 bool wl_doppler_length(int n);
 int wl_doppler_columns(int n);
 int wl_doppler_box_rows(int n);
-int launch_doppler_worklist(const WlDopplerParams& p, int ctas, cudaStream_t stream);
+int launch_doppler_worklist(const WlDopplerParams& p, int ctas, int cls, cudaStream_t stream);
 
-// CFAR window geometries with the tiled kernel, the tile's halo box (floats), and the launch.
+// CFAR window geometries with the tiled kernel, the tile's halo box (floats), and the launch
+// over `tiles` entries (persistent CTAs, two halo buffers each).
 bool wl_cfar_geometry(int gr, int gc, int rr, int rc, uint32_t* box_w, uint32_t* box_h);
-int launch_cfar_worklist(const WlCfarParams& p, int ctas, int gr, int gc, int rr, int rc, cudaStream_t stream);
+int launch_cfar_worklist(const WlCfarParams& p, int tiles, int gr, int gc, int rr, int rc, cudaStream_t stream);
 
 }  // namespace zkx
