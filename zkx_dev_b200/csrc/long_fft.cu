@@ -153,6 +153,93 @@ __device__ __forceinline__ void cross_natural_scatter(const cg::cluster_group& c
     }
 }
 
+// Twiddles of the cross-CTA passes of one CTA of the persistent kernel, the same for every
+// pulse it transforms.  Forward pass: W_N^(n2 k1) for n2 = c S + t + T j is
+// base[k1 - 1] * step[j (R - 1) + k1 - 1] with base = W_N^((c S + t) k1) per thread and
+// step = W_N^(T j k1) shared.  Inverse pass of CTA k1: W_N^(-m k1) for m = t + T r is
+// ibase * istep[r] with ibase = W_N^(-t k1), istep = W_N^(-T r k1).  One complex product
+// replaces a table load per value (the product differs from the table value by about one
+// unit in the last place).
+template <int R>
+struct CrossTwiddles {
+    static constexpr int PER = kM / R / kT;
+    static constexpr int STEP = PER * (R - 1);   // forward steps
+    static constexpr int WORDS = STEP + kE;       // shared words (forward + inverse steps)
+    float2 base[R - 1];
+    float2 ibase;
+};
+
+// Fill the shared steps (all threads) and this thread's bases.
+template <int R>
+__device__ __forceinline__ void cross_twiddles_init(CrossTwiddles<R>& c, float2* steps, int k1, int t,
+                                                    const float2* __restrict__ tw)
+{
+    using CT = CrossTwiddles<R>;
+    for (int i = t; i < CT::STEP; i += kT) {
+        const int j = i / (R - 1), k = i - j * (R - 1) + 1;
+        steps[i] = long_twiddle<R, -1>(tw, kT * j * k);
+    }
+    for (int r = t; r < kE; r += kT) steps[CT::STEP + r] = long_twiddle<R, 1>(tw, kT * r * k1);
+#pragma unroll
+    for (int k = 1; k < R; ++k) c.base[k - 1] = long_twiddle<R, -1>(tw, (k1 * (kM / R) + t) * k);
+    c.ibase = long_twiddle<R, 1>(tw, t * k1);
+}
+
+// cross_dif_scatter (forward, DIR -1) with the twiddles of cross_twiddles_init.
+template <int R, class Load>
+__device__ __forceinline__ void cross_dif_scatter_tw(const cg::cluster_group& cl, float2* sm, int c, int t,
+                                                     const CrossTwiddles<R>& ct, const float2* steps, Load load)
+{
+    constexpr int S = kM / R, PER = S / kT;
+    uint32_t dst[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) dst[k] = cluster_address(sm, k);
+    cl.sync();  // every CTA of the cluster is running before its shared memory is written
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        const int n2 = c * S + t + kT * j;
+        float2 a[R];
+#pragma unroll
+        for (int n1 = 0; n1 < R; ++n1) a[n1] = load(n1 * kM + n2);
+        dft<R, -1>(a);
+        store_cluster(dst[0] + 8u * n2, a[0]);
+#pragma unroll
+        for (int k1 = 1; k1 < R; ++k1)
+            store_cluster(dst[k1] + 8u * n2, cmul(a[k1], cmul(ct.base[k1 - 1], steps[j * (R - 1) + k1 - 1])));
+    }
+    cl.sync();  // all of this CTA's b values have arrived
+}
+
+// cross_dit_gather (inverse, DIR +1, unscaled) with the twiddles of cross_twiddles_init.
+template <int R>
+__device__ __forceinline__ void cross_dit_gather_tw(const cg::cluster_group& cl, const float2 (&v)[kE], float2* sm,
+                                                    int k1, int t, const CrossTwiddles<R>& ct, const float2* steps,
+                                                    float2* yr)
+{
+    constexpr int S = kM / R, PER = S / kT;
+    const float2* istep = steps + CrossTwiddles<R>::STEP;
+    uint32_t dst[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) dst[k] = cluster_address(sm, k);
+    cl.sync();  // every CTA has finished its local transform: exchange buffers are free
+#pragma unroll
+    for (int r = 0; r < kE; ++r) {
+        const float2 zv = k1 ? cmul(v[r], cmul(ct.ibase, istep[r])) : v[r];
+        store_cluster(dst[r / PER] + 8u * (k1 * S + t + kT * (r % PER)), zv);
+    }
+    cl.sync();
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        const int mm = t + kT * j;
+        float2 a[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k) a[k] = sm[k * S + mm];
+        dft<R, 1>(a);
+#pragma unroll
+        for (int c = 0; c < R; ++c) yr[(size_t)c * kM + k1 * S + mm] = a[c];
+    }
+}
+
 // v[r] = sm[t + T r], then a block barrier so the local transform may reuse sm.
 __device__ __forceinline__ void take_own(float2 (&v)[kE], const float2* sm, int t)
 {
@@ -263,8 +350,10 @@ long_compression_kernel(const Src src, int pulses, int samples,
 // in the digit-reversed order that ordering leaves in registers (tcgen05.st once,
 // tcgen05.ld per pulse: 256 columns, one CTA per SM).  At the start of each pulse every
 // CTA pulls its slice of the cluster's next pulse into L2, so that pulse's cross-CTA pass
-// reads L2.  The cross-CTA passes are the same as above; their cluster barriers also order
-// one pulse's last reads of shared memory before the next pulse's remote writes.
+// reads L2.  The cross-CTA passes are those above with their twiddles formed from
+// per-thread bases and shared steps set up once (CrossTwiddles) instead of table loads per
+// value; their cluster barriers also order one pulse's last reads of shared memory before
+// the next pulse's remote writes.
 template <int R, class Src>
 __global__ void __cluster_dims__(R, 1, 1) __launch_bounds__(kT, 1)
 long_compression_local_kernel(const Src src, int pulses, int samples, const float2* __restrict__ spectrum,
@@ -290,6 +379,9 @@ long_compression_local_kernel(const Src src, int pulses, int samples, const floa
         tmem_relinquish();
     }
     float2* first = tab + LP::TABLE + t * (LOGE | 1);
+    float2* steps = tab + LP::TABLE + kT * (LOGE | 1);   // CrossTwiddles<R>::WORDS
+    CrossTwiddles<R> ct;
+    cross_twiddles_init<R>(ct, steps, k1, t, tw);
     fill_local_table<LP>(tab, t, kT, tw);
     {
         float2 wb[LOGE];
@@ -316,14 +408,14 @@ long_compression_local_kernel(const Src src, int pulses, int samples, const floa
                 bulk_prefetch_l2(nx + lo, (uint32_t)(hi - lo) * (uint32_t)sizeof(float2));
         }
         const float2* xr = src.row(pulse);
-        cross_dif_scatter<R, -1>(cl, sm, k1, t, tw,
-                                 [&](int e) { return e < avail ? __ldcs(&xr[e]) : make_float2(0.f, 0.f); });
+        cross_dif_scatter_tw<R>(cl, sm, k1, t, ct, steps,
+                                [&](int e) { return e < avail ? __ldcs(&xr[e]) : make_float2(0.f, 0.f); });
         float2 v[kE];
         take_own(v, sm, t);
         local_fft_forward<LP>(v, sm, t, twiddle, tab);
         tmem_multiply<kE, false>(v, spec_cols);
         local_fft_inverse<LP>(v, sm, t, twiddle_conj, tab);
-        cross_dit_gather<R, 1>(cl, v, sm, k1, t, tw, y + (size_t)pulse * N, 1.0f);
+        cross_dit_gather_tw<R>(cl, v, sm, k1, t, ct, steps, y + (size_t)pulse * N);
     }
     tc_fence_before();
     __syncthreads();
@@ -376,7 +468,8 @@ int replica_long(const float2* h, int length, int normalize, int kind, const flo
 }
 
 constexpr size_t kLocalSmemBytes =
-    ((size_t)LocalPlan<kM>::EXCHANGE + 2 + LocalPlan<kM>::TABLE + (size_t)kT * (ilog2(kE) | 1)) * sizeof(float2);
+    ((size_t)LocalPlan<kM>::EXCHANGE + 2 + LocalPlan<kM>::TABLE + (size_t)kT * (ilog2(kE) | 1) +
+     (size_t)std::max(CrossTwiddles<2>::WORDS, CrossTwiddles<4>::WORDS)) * sizeof(float2);
 
 // Clusters of the persistent kernel resident on the GPU at once.
 template <int R>
