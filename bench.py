@@ -175,32 +175,54 @@ def run_ours(args, rank: int, world: int, dist) -> dict:
         LB.check(lib.zkx_resample_poly_f32(fir_out.data_ptr(), CH, NS, ctypes.byref(lay),
                                            taps_rs.data_ptr(), rs_out.data_ptr(), h))
 
-    # A step: the front end (FIR, resample_poly) and the range-Doppler chain are independent,
-    # so the front end runs on its own stream beside the chain (each fills the other's
-    # partial waves); the next step starts once both are done.
+    # A step: the front end (FIR, resample_poly) and the range-Doppler chain of one CPI; the
+    # two are independent, so the front end runs on its own stream beside the chain (each
+    # fills the other's partial waves).  Two steps are in flight: step i runs on lane i % 2
+    # (a front-end stream, a chain stream and its own output buffers), so step i+1's kernels
+    # also fill the waves step i's leave partly empty; step i+2 reuses step i's lane, whose
+    # stream order protects its buffers.
     fe_stream = torch.cuda.Stream(device=dev)
     fe_sh = fe_stream.cuda_stream
     fe_events = [torch.cuda.Event() for _ in range(4)]
+    lanes = 2
+    lane_chain = [torch.cuda.Stream(device=dev) for _ in range(lanes)]
+    lane_fe = [torch.cuda.Stream(device=dev) for _ in range(lanes)]
+    lane_out = [out] + [chain.allocate_outputs() for _ in range(lanes - 1)]
+    lane_fir = [fir_out] + [torch.empty_like(fir_out) for _ in range(lanes - 1)]
+    lane_rs = [rs_out] + [torch.empty_like(rs_out) for _ in range(lanes - 1)]
 
     def step(i):
-        k = i % n_sets
-        start, done = fe_events[2 * (i % 2)], fe_events[2 * (i % 2) + 1]
-        start.record(stream)
-        fe_stream.wait_event(start)
+        k, ln = i % n_sets, i % lanes
+        h = lane_fe[ln].cuda_stream
         LB.check(lib.zkx_fir_f32(taps_fir.data_ptr(), FIR_TAPS, dev_fe[k].data_ptr(), CH, NS, None,
-                                 fir_out.data_ptr(), None, fe_sh))
-        LB.check(lib.zkx_resample_poly_f32(fir_out.data_ptr(), CH, NS, ctypes.byref(lay),
-                                           taps_rs.data_ptr(), rs_out.data_ptr(), fe_sh))
-        done.record(fe_stream)
-        chain(dev_cube[k], out)
-        stream.wait_event(done)
+                                 lane_fir[ln].data_ptr(), None, h))
+        LB.check(lib.zkx_resample_poly_f32(lane_fir[ln].data_ptr(), CH, NS, ctypes.byref(lay),
+                                           taps_rs.data_ptr(), lane_rs[ln].data_ptr(), h))
+        with torch.cuda.stream(lane_chain[ln]):
+            chain(dev_cube[k], lane_out[ln])
+
+    def lanes_begin():
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        for s_ in lane_chain + lane_fe:
+            s_.wait_event(ev)
+
+    def lanes_end():
+        for s_ in lane_chain + lane_fe:
+            ev = torch.cuda.Event()
+            ev.record(s_)
+            stream.wait_event(ev)
 
     # warm-up
+    lanes_begin()
     for i in range(args.warmup):
         step(i)
+    lanes_end()
     torch.cuda.synchronize()
     if args.profile:
+        lanes_begin()
         step(0)
+        lanes_end()
         torch.cuda.synchronize()
         chain.close()
         return None
@@ -241,8 +263,10 @@ def run_ours(args, rank: int, world: int, dist) -> dict:
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
+    lanes_begin()
     for i in range(args.steps):
         step(i)
+    lanes_end()
     t1.record(stream)
     torch.cuda.synchronize()
     if dist is not None:

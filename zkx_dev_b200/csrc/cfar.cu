@@ -241,7 +241,9 @@ struct CfarTmaGeom {
 
 // Vertical pieces of a staged 64 x 64 tile: one item per (halo column, 32-row segment), a
 // round of the CTA's threads for the 2/8 window (84 halo columns x 2 segments); longer
-// segments sum fewer halo rows per cell.
+// segments sum fewer halo rows per cell.  (Three segments of 22/21/21 rows, which keep 252
+// of the 256 threads busy instead of 168, measured slower: 260.2 against 253.5 us for the
+// 1024 x 16384 chain.)
 template <int GR, int GC, int RR, int RC>
 __device__ __forceinline__ void full_tile_vertical(const float* P, float* SA, float* SB)
 {
