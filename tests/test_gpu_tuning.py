@@ -233,3 +233,47 @@ def test_tuning_rejects_unknown_choices(z):
                {"cfar_tile": 4}, {"compression_variant": 4}):
         t = L.RdTuning(**kw)
         assert L.lib().zkx_rd_plan_set_tuning(chain._plan, ctypes.byref(t)) == L.INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("P,N", [(2048, 1024), (4096, 512), (1500, 640)])
+def test_long_doppler_tiles_match(z, P, N):
+    """Slow-time transforms of 2048 and 4096 bins on the bulk-copy tiles, on 16-byte-misaligned
+    input (the per-thread-load kernel) and against the FP64 DFT: the same bits on both paths,
+    within FP32 rounding of FP64; both tile widths of the chain give the same bits."""
+    import oracle as O
+    from zkx_dev_b200 import _lib as L
+    rng = np.random.default_rng(P + N)
+    xh = (rng.standard_normal((P, N)) + 1j * rng.standard_normal((P, N))).astype(np.complex64)
+    nfft = 1 << (P - 1).bit_length()
+    buf = torch.empty(P * N + 1, dtype=torch.complex64, device="cuda")
+    mis = buf[1:].view(P, N)
+    mis.copy_(torch.as_tensor(xh).cuda())
+    x = torch.as_tensor(xh).cuda()
+    outs = []
+    for src in (x, mis):
+        rd = torch.empty((nfft, N), dtype=torch.complex64, device="cuda")
+        pw = torch.empty((nfft, N), dtype=torch.float32, device="cuda")
+        L.check(L.lib().zkx_pulse_doppler_c64(src.data_ptr(), P, N, nfft, L.WINDOW_HAMMING, None, rd.data_ptr(),
+                                              pw.data_ptr(), L.stream_handle()))
+        torch.cuda.synchronize()
+        outs.append((rd.cpu(), pw.cpu()))
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+    cols = [0, N // 2, N - 1]
+    rd64, _ = O.pulse_doppler_fft64(xh[:, cols], nfft, O.radar_window_f32("hamming", P))
+    got = outs[0][0].numpy()[:, cols].astype(np.complex128)
+    assert np.linalg.norm(got - rd64) / np.linalg.norm(rd64) <= 1e-5
+    # the chain with each tile width
+    from zkx_dev_b200.synth import make_cpi
+    cpi = make_cpi(P, N, 5, 64, seed=P)
+    chain = z.RangeDopplerChain(z.ChainConfig(P, N, 64, doppler_nfft=nfft), torch.as_tensor(cpi.replica).cuda())
+    wide = 8 if nfft == 2048 else 4
+    res = []
+    for c in (0, wide, wide // 2):     # 0: by shape (per-thread loads at 4096 bins)
+        set_full_tuning(chain, doppler_columns=c)
+        o = chain(torch.as_tensor(cpi.x).cuda())
+        torch.cuda.synchronize()
+        res.append({k: o[k].clone() for k in ("rd", "power", "detections")})
+    for r in res[1:]:
+        for k in res[0]:
+            assert torch.equal(res[0][k], r[k]), k
+    assert L.kernel_status(clear=True) == 0

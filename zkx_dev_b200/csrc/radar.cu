@@ -730,6 +730,21 @@ int doppler_impl(const float2* x, int pulses, int samples, const float* window, 
                 return ct == 8 ? doppler_tma<N, 8>(map, pulses, samples, window, out, power, batch, s)
                                : doppler_tma<N, 16>(map, pulses, samples, window, out, power, batch, s);
         }
+    } else if constexpr (N == 2048 || N == 4096) {
+        // the longest slow-time transforms in one CTA: narrower bulk-copy tiles (C = 4 or 8
+        // columns at 2048 pulses, 2 or 4 at 4096; 64-147 KB), the same tile code.  By shape
+        // at 2048 (4 columns; 2048 x 65536: 1091 against 1246 us with per-thread loads), only
+        // when tuned at 4096 (2 columns: 430 against 373 us at 4096 x 8192)
+        const bool tuned = columns != 0;
+        if ((samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0 && (N == 2048 || tuned)) {
+            constexpr int NARROW = N == 2048 ? 4 : 2;
+            const int ct = columns == 2 * NARROW ? 2 * NARROW : NARROW;
+            CUtensorMap map;
+            if (encode_tensor_map_2d_f32(&map, x, 2ull * samples, (uint64_t)pulses * batch,
+                                         (uint64_t)samples * sizeof(float2), 2 * ct, 256))
+                return ct == NARROW ? doppler_tma<N, NARROW>(map, pulses, samples, window, out, power, batch, s)
+                                    : doppler_tma<N, 2 * NARROW>(map, pulses, samples, window, out, power, batch, s);
+        }
     }
     const size_t smem = (size_t)C * PL::smem_elems(C < 16) * sizeof(float2);
     if (smem > 227 * 1024)  // the column tile does not fit: transposed row passes instead
