@@ -450,7 +450,7 @@ enum {
 typedef struct {
     int compression_variant;  /* ZKX_COMPRESSION_* */
     int doppler_columns;      /* range columns per CTA of the bulk-copy Doppler kernel: 8 or 16
-                                 (4 or 8 at 2048 Doppler bins; 2 or 4 at 4096, whose default is
+                                 (4 or 8 at 2048 Doppler bins; 2 or 4 at 4096, where 1 selects
                                  the per-thread-load kernel) */
     int cfar_tile;            /* ZKX_CFAR_TILE_* (accurate-mode CA-CFAR of the tiled window sizes) */
     int compression_radix;    /* values per thread (radix plan) of the Stockham compression kernels

@@ -266,9 +266,8 @@ def test_long_doppler_tiles_match(z, P, N):
     from zkx_dev_b200.synth import make_cpi
     cpi = make_cpi(P, N, 5, 64, seed=P)
     chain = z.RangeDopplerChain(z.ChainConfig(P, N, 64, doppler_nfft=nfft), torch.as_tensor(cpi.replica).cuda())
-    wide = 8 if nfft == 2048 else 4
     res = []
-    for c in (0, wide, wide // 2):     # 0: by shape (per-thread loads at 4096 bins)
+    for c in ((0, 8, 4) if nfft == 2048 else (0, 4, 2, 1)):   # 0: by shape; 1: per-thread loads
         set_full_tuning(chain, doppler_columns=c)
         o = chain(torch.as_tensor(cpi.x).cuda())
         torch.cuda.synchronize()

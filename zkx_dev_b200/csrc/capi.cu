@@ -710,10 +710,10 @@ extern "C" int zkx_rd_plan_autotune(zkx_rd_plan p, const void* x, int batch, zkx
     }
     if (rc == ZKX_SUCCESS) {
         float tbest = 0.f;
-        // bulk-copy tile widths: 16 or 8 columns, 8 or 4 at 2048 pulses; at 4096 the
-        // per-thread-load kernel (0, the shape's default) or bulk-copy tiles of 4 or 2
+        // bulk-copy tile widths: 16 or 8 columns; 8 or 4 at 2048 pulses; 4 or 2 at 4096,
+        // or its per-thread-load kernel (1)
         std::vector<int> widths = nd == 2048 ? std::vector<int>{8, 4}
-                                  : nd == 4096 ? std::vector<int>{0, 4, 2} : std::vector<int>{16, 8};
+                                  : nd == 4096 ? std::vector<int>{4, 2, 1} : std::vector<int>{16, 8};
         for (int c : widths) {
             float ms = 0.f;
             rc = time_median([&] {
@@ -786,8 +786,8 @@ extern "C" int zkx_rd_plan_set_tuning(zkx_rd_plan p, const zkx_rd_tuning* t)
 {
     if (!p || !t) return fail(ZKX_INVALID_ARGUMENT, "rd_plan_set_tuning: null pointer");
     if (t->compression_variant < 0 || t->compression_variant > ZKX_COMPRESSION_LOCAL ||
-        (t->doppler_columns != 0 && t->doppler_columns != 2 && t->doppler_columns != 4 &&
-         t->doppler_columns != 8 && t->doppler_columns != 16) ||
+        (t->doppler_columns != 0 && t->doppler_columns != 1 && t->doppler_columns != 2 &&
+         t->doppler_columns != 4 && t->doppler_columns != 8 && t->doppler_columns != 16) ||
         t->cfar_tile < 0 || t->cfar_tile > ZKX_CFAR_TILE_STREAM ||
         (t->compression_radix != 0 && t->compression_radix != 16 && t->compression_radix != 32) ||
         t->compression_ctas_per_sm < 0 || t->compression_ctas_per_sm > 32 || t->cfar_ctas_per_sm < 0 ||

@@ -732,13 +732,12 @@ int doppler_impl(const float2* x, int pulses, int samples, const float* window, 
         }
     } else if constexpr (N == 2048 || N == 4096) {
         // the longest slow-time transforms in one CTA: narrower bulk-copy tiles (C = 4 or 8
-        // columns at 2048 pulses, 2 or 4 at 4096; 64-147 KB), the same tile code.  By shape
-        // at 2048 (4 columns; 2048 x 65536: 1091 against 1246 us with per-thread loads), only
-        // when tuned at 4096 (2 columns: 430 against 373 us at 4096 x 8192)
-        const bool tuned = columns != 0;
-        if ((samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0 && (N == 2048 || tuned)) {
+        // columns at 2048 pulses, 2 or 4 at 4096; 64-147 KB), the same tile code.  By shape:
+        // 4 columns (chain 2048 x 16384: 474 us against 503 with 8; 4096 x 8192: 541 us
+        // against 549 with 2 and 606 with per-thread loads, which the tuning value 1 keeps)
+        if ((samples & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0 && columns != 1) {
             constexpr int NARROW = N == 2048 ? 4 : 2;
-            const int ct = columns == 2 * NARROW ? 2 * NARROW : NARROW;
+            const int ct = columns == NARROW || columns == 2 * NARROW ? columns : 4;
             CUtensorMap map;
             if (encode_tensor_map_2d_f32(&map, x, 2ull * samples, (uint64_t)pulses * batch,
                                          (uint64_t)samples * sizeof(float2), 2 * ct, 256))

@@ -88,7 +88,7 @@ int launch_pulse_compression_variant(const float2* x, int pulses, int samples, i
                                      const float2* spectrum, float2* y, int variant, cudaStream_t stream,
                                      int radix = 0, int ctas_per_sm = 0);
 // columns: range columns per CTA of the bulk-copy Doppler kernel (8 or 16; 4 or 8 at 2048
-// pulses, 2 or 4 at 4096; 0 = by shape).
+// pulses, 2 or 4 at 4096, where 1 selects the per-thread-load kernel; 0 = by shape).
 int launch_pulse_doppler(const float2* x, int pulses, int samples, int nfft,
                          const float* window, float2* out, float* power, int batch, int columns,
                          cudaStream_t stream);
