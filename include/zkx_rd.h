@@ -500,8 +500,11 @@ ZKX_API int zkx_rd_graph_destroy(zkx_rd_graph graph);
  * stage with its own kernels, one launch per plan (per CPI for CFAR).  Every CPI's
  * threshold and detections equal zkx_rd_execute of that CPI alone with its plan, bit for
  * bit, and so does its power plane, copied to `power` when that is not NULL.  Plans must
- * have FP32 precision; items must stay valid (and the plans alive) until destroy.  launch
- * may be captured into a CUDA graph.  count: 1 .. 65535. */
+ * have FP32 precision; items must stay valid (and the plans alive) until destroy.  The
+ * kernel choices are taken from the plans' tunings at create (a later tuning change needs a
+ * new list).  Launches of one list share its library-owned buffers, so they must be ordered
+ * (one stream, or events between streams).  launch may be captured into a CUDA graph.
+ * count: 1 .. 65535. */
 typedef struct zkx_rd_worklist_s* zkx_rd_worklist;
 typedef struct {
     zkx_rd_plan plan;
