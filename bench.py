@@ -184,8 +184,13 @@ def run_ours(args, rank: int, world: int, dist) -> dict:
     fe_sh = fe_stream.cuda_stream
     fe_events = [torch.cuda.Event() for _ in range(4)]
     lanes = max(1, args.lanes)
-    lane_chain = [torch.cuda.Stream(device=dev) for _ in range(lanes)]
-    lane_fe = [torch.cuda.Stream(device=dev) for _ in range(lanes)]
+    # the chain's streams get the device's highest scheduling priority and the front end's the
+    # lowest (unless --equal-priority), so pending chain CTAs are placed first and the front
+    # end fills what the chain leaves
+    lo, hi = torch.cuda.Stream.priority_range()
+    prio = not args.equal_priority
+    lane_chain = [torch.cuda.Stream(device=dev, priority=hi if prio else 0) for _ in range(lanes)]
+    lane_fe = [torch.cuda.Stream(device=dev, priority=lo if prio else 0) for _ in range(lanes)]
     lane_out = [out] + [chain.allocate_outputs() for _ in range(lanes - 1)]
     lane_fir = [fir_out] + [torch.empty_like(fir_out) for _ in range(lanes - 1)]
     lane_rs = [rs_out] + [torch.empty_like(rs_out) for _ in range(lanes - 1)]
@@ -1000,6 +1005,10 @@ def main() -> None:
                     help="steps in flight, each on its own front-end and chain streams and buffers "
                          "(2 measured slower over 1000 steps: 0.331 against 0.314 ms per step, the "
                          "other step's traffic evicting the compressed cube Doppler reads from L2)")
+    ap.add_argument("--equal-priority", action="store_true",
+                    help="run the chain's and the front end's streams at the same scheduling priority "
+                         "(default: the chain's highest, the front end's lowest; 0.3134 against 0.3146 ms "
+                         "per step over 1000 steps)")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the mixed-stream serving measurement")
