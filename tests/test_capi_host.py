@@ -141,3 +141,21 @@ def test_wait_timeout_selftest_checks_its_limit(L):
     device work (so this runs without a GPU)."""
     for bad in (0, 999, (1 << 31) + 1):
         assert L.lib().zkx_selftest_wait_timeout(bad, None) == L.INVALID_ARGUMENT
+
+
+def test_worklist_and_tuning_validation_codes(L):
+    """The work list and the plan-tuning entries reject null and out-of-range arguments with
+    the reference's codes before any device work."""
+    lib = L.lib()
+    h = ctypes.c_void_p()
+    assert lib.zkx_rd_worklist_create(None, 1, ctypes.byref(h)) == L.INVALID_ARGUMENT
+    items = (L.WorkItem * 1)()
+    assert lib.zkx_rd_worklist_create(items, 1, None) == L.INVALID_ARGUMENT
+    assert lib.zkx_rd_worklist_create(items, 0, ctypes.byref(h)) == L.INVALID_SHAPE
+    assert lib.zkx_rd_worklist_create(items, 70000, ctypes.byref(h)) == L.INVALID_SHAPE
+    assert lib.zkx_rd_worklist_launch(None, None) == L.INVALID_ARGUMENT
+    assert lib.zkx_rd_worklist_info(None, None, None, None) == L.INVALID_ARGUMENT
+    assert lib.zkx_rd_worklist_destroy(None) == L.SUCCESS
+    t = L.RdTuning()
+    assert lib.zkx_rd_plan_set_tuning(None, ctypes.byref(t)) == L.INVALID_ARGUMENT
+    assert lib.zkx_rd_plan_get_tuning(None, ctypes.byref(t)) == L.INVALID_ARGUMENT
