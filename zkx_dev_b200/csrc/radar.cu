@@ -1032,7 +1032,7 @@ int wl_length_class(int n)
 int wl_compression_ctas(int n, int rows)
 {
     const int per = kWlCompressionThreads / (n / elems_for(n));
-    return (rows + per - 1) / per;
+    return (int)(((long long)rows + per - 1) / per);
 }
 
 template <int CLASS>

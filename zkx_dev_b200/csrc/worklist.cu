@@ -128,7 +128,9 @@ int build_params(zkx_rd_worklist w)
     for (int cls : {0, 1})
     for (WlGroup& g : w->groups) {
         if (!g.comp_wl || wl_length_class(g.v.range_nfft) != cls) continue;
-        if (w->comp.empty() || w->comp.back().groups == kWlGroups || w->comp.back().cls != cls) {
+        const long long add = wl_compression_ctas(g.v.range_nfft, g.count * g.v.d.num_pulses);
+        if (w->comp.empty() || w->comp.back().groups == kWlGroups || w->comp.back().cls != cls ||
+            w->comp_ctas.back() + add > INT_MAX) {
             w->comp.emplace_back();
             std::memset(&w->comp.back(), 0, sizeof(WlCompressionParams));
             w->comp.back().cls = cls;
@@ -144,7 +146,7 @@ int build_params(zkx_rd_worklist w)
         e.nfft = g.v.range_nfft;
         e.rows = g.count * g.v.d.num_pulses;
         e.entry0 = w->comp_ctas.back();
-        w->comp_ctas.back() += wl_compression_ctas(e.nfft, e.rows);
+        w->comp_ctas.back() += (int)add;
     }
 
     for (int cls : {0, 1})
@@ -158,7 +160,10 @@ int build_params(zkx_rd_worklist w)
             g.dop_wl = false;  // the plan's own Doppler launch instead
             continue;
         }
-        if (w->dop.empty() || w->dop.back().groups == kWlGroups || w->dop.back().cls != cls) {
+        const long long add = (long long)g.count * ((nr + C - 1) / C);
+        if (add > INT_MAX) return fail(ZKX_INVALID_SHAPE, "rd_worklist_create: a plan's Doppler tiles exceed one launch");
+        if (w->dop.empty() || w->dop.back().groups == kWlGroups || w->dop.back().cls != cls ||
+            w->dop_ctas.back() + add > INT_MAX) {
             w->dop.emplace_back();
             std::memset(&w->dop.back(), 0, sizeof(WlDopplerParams));
             w->dop.back().cls = cls;
@@ -174,7 +179,7 @@ int build_params(zkx_rd_worklist w)
         e.nd = nd;
         e.tiles_x = (nr + C - 1) / C;
         e.entry0 = w->dop_ctas.back();
-        w->dop_ctas.back() += g.count * e.tiles_x;
+        w->dop_ctas.back() += (int)add;
     }
 
     for (WlGroup& g : w->groups) {
@@ -189,7 +194,9 @@ int build_params(zkx_rd_worklist w)
             g.cfar_wl = false;
             continue;
         }
-        if (w->cfar.empty() || w->cfar.back().groups == kWlGroups) {
+        const long long add = (long long)g.count * ((nr + 63) / 64) * ((nd + 63) / 64);
+        if (add > INT_MAX) return fail(ZKX_INVALID_SHAPE, "rd_worklist_create: a plan's CFAR tiles exceed one launch");
+        if (w->cfar.empty() || w->cfar.back().groups == kWlGroups || w->cfar_ctas.back() + add > INT_MAX) {
             w->cfar.emplace_back();
             std::memset(&w->cfar.back(), 0, sizeof(WlCfarParams));
             w->cfar_ctas.push_back(0);
@@ -206,7 +213,7 @@ int build_params(zkx_rd_worklist w)
         e.tiles_x = (nr + 63) / 64;
         e.tiles_y = (nd + 63) / 64;
         e.entry0 = w->cfar_ctas.back();
-        w->cfar_ctas.back() += g.count * e.tiles_x * e.tiles_y;
+        w->cfar_ctas.back() += (int)add;
     }
 
     // launch calls per run
