@@ -149,7 +149,9 @@ def test_pulse_doppler_full_size_sampled_columns(z):
 
 @pytest.mark.parametrize("shape,guard,train", [((64, 96), (2, 2), (8, 8)), ((40, 50), (1, 1), (4, 4)),
                                                ((128, 4096), (2, 2), (8, 8)), ((33, 70), (2, 2), (4, 4)),
-                                               ((30, 31), (1, 2), (3, 5)), ((16, 16), (1, 1), (4, 4))])
+                                               ((30, 31), (1, 2), (3, 5)), ((16, 16), (1, 1), (4, 4)),
+                                               # Task1's window (task1_selected.conf): a tiled geometry
+                                               ((128, 512), (1, 2), (2, 6)), ((300, 1000), (1, 2), (2, 6))])
 def test_ca_cfar_accurate_mask_equals_fp64(z, shape, guard, train):
     rng = np.random.default_rng(shape[0] * shape[1])
     p = rng.exponential(size=shape).astype(np.float32)

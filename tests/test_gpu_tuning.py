@@ -276,3 +276,25 @@ def test_long_doppler_tiles_match(z, P, N):
         for k in res[0]:
             assert torch.equal(res[0][k], r[k]), k
     assert L.kernel_status(clear=True) == 0
+
+
+def test_cfar_tiles_on_task1_window(z):
+    """Task1's CA-CFAR window (guard 1 x 2, reference 2 x 6) runs the tiled kernels: every tile
+    choice gives the FP64 CFAR's mask, the full and persistent tiles the same thresholds."""
+    import oracle as O
+    from zkx_dev_b200.synth import make_cpi
+    P, N = 128, 4096
+    cpi = make_cpi(P, N, 12, 256, seed=77)
+    chain = z.RangeDopplerChain(z.ChainConfig(P, N, 256, guard_cells=(1, 2), reference_cells=(2, 6), pfa=1e-4),
+                                torch.as_tensor(cpi.replica).cuda())
+    x = torch.as_tensor(cpi.x).cuda()
+    outs = {}
+    for tile in (1, 2, 3):
+        set_tuning(chain, 0, 0, tile)
+        o = chain(x)
+        torch.cuda.synchronize()
+        outs[tile] = {k: o[k].cpu().numpy().copy() for k in ("power", "threshold", "detections")}
+    _, m64 = O.ca_cfar_f64(outs[1]["power"], (1, 2), (2, 6), 1e-4)
+    for tile in (1, 2, 3):
+        np.testing.assert_array_equal(outs[tile]["detections"], m64)
+    np.testing.assert_array_equal(outs[3]["threshold"], outs[1]["threshold"])

@@ -712,7 +712,9 @@ void cfar_box(uint32_t* w, uint32_t* h)
     *h = (uint32_t)G::HR;
 }
 
-// Any window geometry: one thread per cell, ring summed directly in FP64.
+// Window geometries without a tiled instantiation (the tiled ones: guard x train 2x2/8x8,
+// 1x1/4x4, 2x2/4x4, 1x1/2x2 and Task1's 1x2/2x6): one thread per cell, ring summed directly
+// in FP64.
 __global__ void cfar_generic_kernel(const float* __restrict__ x, int rows, int cols, int gr, int gc,
                                     int rr, int rc, double scale64, float* __restrict__ thr,
                                     uint8_t* __restrict__ det)
@@ -905,6 +907,7 @@ int launch_ca_cfar_accurate(const float* x, int rows, int columns, int gr, int g
     ZKX_CFAR_CASE(1, 1, 4, 4)
     ZKX_CFAR_CASE(2, 2, 4, 4)
     ZKX_CFAR_CASE(1, 1, 2, 2)
+    ZKX_CFAR_CASE(1, 2, 2, 6)
 #undef ZKX_CFAR_CASE
     const long long count = (long long)rows * columns;
     cfar_generic_kernel<<<dim3((unsigned)((count + 255) / 256), batch), 256, 0, stream>>>(
@@ -942,6 +945,7 @@ bool wl_cfar_geometry(int gr, int gc, int rr, int rc, uint32_t* box_w, uint32_t*
     ZKX_CFAR_CASE(1, 1, 4, 4)
     ZKX_CFAR_CASE(2, 2, 4, 4)
     ZKX_CFAR_CASE(1, 1, 2, 2)
+    ZKX_CFAR_CASE(1, 2, 2, 6)
 #undef ZKX_CFAR_CASE
     return false;
 }
@@ -954,6 +958,7 @@ int launch_cfar_worklist(const WlCfarParams& p, int tiles, int gr, int gc, int r
     ZKX_CFAR_CASE(1, 1, 4, 4)
     ZKX_CFAR_CASE(2, 2, 4, 4)
     ZKX_CFAR_CASE(1, 1, 2, 2)
+    ZKX_CFAR_CASE(1, 2, 2, 6)
 #undef ZKX_CFAR_CASE
     return fail(ZKX_UNSUPPORTED_OPERATION, "cfar work list: window geometry without a tiled kernel");
 }
