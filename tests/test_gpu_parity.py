@@ -1,8 +1,8 @@
 """GPU parity: the CUDA kernels (through libzkx_rd.so) against the oracle.
 
-Tolerances: the reference's FP32 path defines parity as relative L2 <= 1e-5 (the
-north-star bar for the plain FP32 path); max relative error against the FP64 oracle is
-checked per output; detection masks are compared exactly.
+Tolerances: parity of the plain FP32 path is relative L2 <= 1e-5 against the reference's
+implementation; max relative error against the FP64 oracle is checked per output;
+detection masks are compared exactly.
 """
 from __future__ import annotations
 
