@@ -545,10 +545,10 @@ typedef struct {
     int reference_cells[2];  /* Doppler, range */
     double pfa;
     int cfar_mode;           /* ZKX_CFAR_ACCURATE or ZKX_CFAR_COMPAT */
-    int streams;             /* compute streams batches are spread over (4); copies use
+    int streams;             /* compute streams batches are spread over (2); copies use
                                 one copy-in and one copy-out stream besides */
     int max_inflight;        /* batches on the device at once (2 * streams) */
-    int max_batch;           /* CPIs of one shape fused into one batch (16, at most 64) */
+    int max_batch;           /* CPIs of one shape fused into one batch (32, at most 64) */
     double hbm_fraction;     /* budget = this fraction of the free HBM at creation (0.8) */
     size_t budget_bytes;     /* nonzero: a lower cap on the budget */
     int max_pending;         /* submitted requests waiting for admission (0 = no bound); a

@@ -25,9 +25,9 @@ class ServerConfig:
     reference_cells: Sequence[int] = (8, 8)
     pfa: float = 1e-6
     cfar_mode: str = "accurate"
-    streams: int = 4
+    streams: int = 2
     max_inflight: int = 0      # 0: 2 * streams
-    max_batch: int = 16
+    max_batch: int = 32
     hbm_fraction: float = 0.8
     budget_bytes: int = 0      # 0: no cap below hbm_fraction of free HBM
     max_pending: int = 0       # 0: unbounded queue; else submits beyond it raise ZkxError 3002
