@@ -151,7 +151,12 @@ def test_pulse_doppler_full_size_sampled_columns(z):
                                                ((128, 4096), (2, 2), (8, 8)), ((33, 70), (2, 2), (4, 4)),
                                                ((30, 31), (1, 2), (3, 5)), ((16, 16), (1, 1), (4, 4)),
                                                # Task1's window (task1_selected.conf): a tiled geometry
-                                               ((128, 512), (1, 2), (2, 6)), ((300, 1000), (1, 2), (2, 6))])
+                                               ((128, 512), (1, 2), (2, 6)), ((300, 1000), (1, 2), (2, 6)),
+                                               # other windows: the runtime-geometry tile kernel, and
+                                               # beyond 32 cells the per-cell kernel
+                                               ((200, 300), (0, 0), (1, 1)), ((100, 150), (3, 1), (5, 12)),
+                                               ((128, 512), (4, 4), (16, 16)), ((61, 77), (0, 3), (2, 29)),
+                                               ((80, 100), (1, 1), (33, 2))])
 def test_ca_cfar_accurate_mask_equals_fp64(z, shape, guard, train):
     rng = np.random.default_rng(shape[0] * shape[1])
     p = rng.exponential(size=shape).astype(np.float32)

@@ -712,9 +712,87 @@ void cfar_box(uint32_t* w, uint32_t* h)
     *h = (uint32_t)G::HR;
 }
 
-// Window geometries without a tiled instantiation (the tiled ones: guard x train 2x2/8x8,
-// 1x1/4x4, 2x2/4x4, 1x1/2x2 and Task1's 1x2/2x6): one thread per cell, ring summed directly
-// in FP64.
+// Any window geometry with guard + train up to 32 cells each way: a 32 x 32 tile per CTA,
+// the tile and its halo staged in shared memory once, the training ring summed separably in
+// FP64 (per halo column the training-row and guard-row sums, then per cell the column sums
+// over the window's width), the threshold FP64 * alpha / N.  A cell within 1e-12 of its
+// threshold is re-decided with the ring summed in the FP64 CFAR's own (row, column) order,
+// so the mask equals an FP64 CFAR of the same input.  About (2 RR + 2 GR + 1) + (2 MC + 1 +
+// 2 RC) FP64 adds per cell instead of the ring's (2 MR + 1)(2 MC + 1).
+constexpr int kRtTile = 32;
+constexpr int kRtMaxHalf = 32;
+
+__host__ __device__ constexpr size_t cfar_rt_smem(int mr, int mc)
+{
+    return (size_t)2 * kRtTile * (kRtTile + 2 * mc) * sizeof(double) +
+           (size_t)(kRtTile + 2 * mr) * ((kRtTile + 2 * mc) | 1) * sizeof(float);
+}
+
+__global__ void __launch_bounds__(256)
+cfar_rt_kernel(const float* __restrict__ x, int rows, int cols, int gr, int gc, int rr, int rc,
+               double scale64, float* __restrict__ thr, uint8_t* __restrict__ det)
+{
+    extern __shared__ __align__(16) double dsm[];
+    const int MR = gr + rr, MC = gc + rc;
+    const int HR = kRtTile + 2 * MR, HC = kRtTile + 2 * MC, HP = HC | 1;
+    double* A = dsm;                                  // [32][HC] training-row sums
+    double* B = A + kRtTile * HC;                     // [32][HC] guard-row sums
+    float* P = reinterpret_cast<float*>(B + kRtTile * HC);   // [HR][HP] tile + halo
+    const int r0 = blockIdx.y * kRtTile, c0 = blockIdx.x * kRtTile;
+    x += (size_t)blockIdx.z * rows * cols;
+    thr += (size_t)blockIdx.z * rows * cols;
+    det += (size_t)blockIdx.z * rows * cols;
+    for (int i = threadIdx.x; i < HR * HC; i += blockDim.x) {
+        const int hr = i / HC, hc = i - (i / HC) * HC;
+        const int r = r0 - MR + hr, c = c0 - MC + hc;
+        P[hr * HP + hc] = (r >= 0 && r < rows && c >= 0 && c < cols) ? __ldg(&x[(size_t)r * cols + c]) : 0.f;
+    }
+    __syncthreads();
+    // halo rows of cell row r (tile row): training rows r .. r+RR-1 and r+MR+GR+1 .. r+2MR,
+    // guard rows r+MR-GR .. r+MR+GR
+    for (int i = threadIdx.x; i < kRtTile * HC; i += blockDim.x) {
+        const int r = i / HC, hc = i - (i / HC) * HC;
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < rr; ++k) a += (double)P[(r + k) * HP + hc];
+        for (int k = 0; k < rr; ++k) a += (double)P[(r + MR + gr + 1 + k) * HP + hc];
+        for (int k = -gr; k <= gr; ++k) b += (double)P[(r + MR + k) * HP + hc];
+        A[r * HC + hc] = a;
+        B[r * HC + hc] = b;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kRtTile * kRtTile; i += blockDim.x) {
+        const int r = i / kRtTile, c = i - (i / kRtTile) * kRtTile;
+        const int grow = r0 + r, gcol = c0 + c;
+        if (grow >= rows || gcol >= cols) continue;
+        const float xv = P[(r + MR) * HP + c + MC];
+        float t = 0.f;
+        bool hit;
+        if (grow >= MR && grow < rows - MR && gcol >= MC && gcol < cols - MC) {
+            double ring = 0.0;
+            for (int dc = -MC; dc <= MC; ++dc) ring += A[r * HC + c + MC + dc];
+            for (int dc = -MC; dc < -gc; ++dc) ring += B[r * HC + c + MC + dc];
+            for (int dc = gc + 1; dc <= MC; ++dc) ring += B[r * HC + c + MC + dc];
+            double t64 = scale64 * ring;
+            if (fabs((double)xv - t64) <= 1e-12 * t64) {
+                double s = 0.0;
+                for (int dr = -MR; dr <= MR; ++dr)
+                    for (int dc = -MC; dc <= MC; ++dc)
+                        if (dr < -gr || dr > gr || dc < -gc || dc > gc)
+                            s += (double)P[(r + MR + dr) * HP + c + MC + dc];
+                t64 = scale64 * s;
+            }
+            t = (float)t64;
+            hit = (double)xv > t64;
+        } else {
+            hit = xv > 0.f;
+        }
+        thr[(size_t)grow * cols + gcol] = t;
+        det[(size_t)grow * cols + gcol] = hit ? 1 : 0;
+    }
+}
+
+// Windows wider than 32 cells each way (beyond cfar_rt_kernel's shared memory): one thread
+// per cell, ring summed directly in FP64.
 __global__ void cfar_generic_kernel(const float* __restrict__ x, int rows, int cols, int gr, int gc,
                                     int rr, int rc, double scale64, float* __restrict__ thr,
                                     uint8_t* __restrict__ det)
@@ -909,6 +987,14 @@ int launch_ca_cfar_accurate(const float* x, int rows, int columns, int gr, int g
     ZKX_CFAR_CASE(1, 1, 2, 2)
     ZKX_CFAR_CASE(1, 2, 2, 6)
 #undef ZKX_CFAR_CASE
+    if (gr + rr <= kRtMaxHalf && gc + rc <= kRtMaxHalf) {
+        const size_t smem = cfar_rt_smem(gr + rr, gc + rc);
+        ZKX_CUDA(cudaFuncSetAttribute(cfar_rt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const dim3 grid((columns + kRtTile - 1) / kRtTile, (rows + kRtTile - 1) / kRtTile, batch);
+        cfar_rt_kernel<<<grid, 256, smem, stream>>>(x, rows, columns, gr, gc, rr, rc, s64, threshold, detections);
+        ZKX_LAUNCHED("cfar_rt_kernel");
+        return ZKX_SUCCESS;
+    }
     const long long count = (long long)rows * columns;
     cfar_generic_kernel<<<dim3((unsigned)((count + 255) / 256), batch), 256, 0, stream>>>(
         x, rows, columns, gr, gc, rr, rc, s64, threshold, detections);
