@@ -830,6 +830,8 @@ __global__ void compat_column_cumsum_kernel(const float* __restrict__ x, int row
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= cols) return;
     float run = 0.f;
+    // unrolled so the loads of several rows are in flight ahead of the sequential adds
+#pragma unroll 16
     for (int r = 0; r < rows; ++r) {
         run = __fadd_rn(run, x[(size_t)r * cols + c]);
         cum[(size_t)r * cols + c] = run;
@@ -837,19 +839,32 @@ __global__ void compat_column_cumsum_kernel(const float* __restrict__ x, int row
 }
 
 // One warp per 32 rows; 32 x 32 tiles are staged through shared memory so the
-// sequential row scan still reads and writes HBM in coalesced rows.
+// sequential row scan still reads and writes HBM in coalesced rows.  The next tile's loads
+// are issued into registers before the current tile is scanned, so their latency overlaps
+// the scan's dependent adds.
 __global__ void compat_row_cumsum_kernel(float* __restrict__ cum, int rows, int cols)
 {
     __shared__ float tile[32][33];
     const int lane = threadIdx.x;
     const int r0 = blockIdx.x * 32;
     float run = 0.f;
+    float next[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        const int rr = r0 + i;
+        next[i] = (rr < rows && lane < cols) ? cum[(size_t)rr * cols + lane] : 0.f;
+    }
     for (int c0 = 0; c0 < cols; c0 += 32) {
-        for (int i = 0; i < 32; ++i) {
-            const int rr = r0 + i, cc = c0 + lane;
-            tile[i][lane] = (rr < rows && cc < cols) ? cum[(size_t)rr * cols + cc] : 0.f;
-        }
+#pragma unroll
+        for (int i = 0; i < 32; ++i) tile[i][lane] = next[i];
         __syncwarp();
+        if (c0 + 32 < cols) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const int rr = r0 + i, cc = c0 + 32 + lane;
+                next[i] = (rr < rows && cc < cols) ? cum[(size_t)rr * cols + cc] : 0.f;
+            }
+        }
         for (int j = 0; j < 32 && c0 + j < cols; ++j) {
             run = __fadd_rn(run, tile[lane][j]);
             tile[lane][j] = run;
