@@ -841,7 +841,7 @@ __global__ void compat_column_cumsum_kernel(const float* __restrict__ x, int row
 // One warp per 32 rows; 32 x 32 tiles are staged through shared memory so the
 // sequential row scan still reads and writes HBM in coalesced rows.  The next tile's loads
 // are issued into registers before the current tile is scanned, so their latency overlaps
-// the scan's dependent adds.
+// the scan's dependent adds, which run on registers.
 __global__ void compat_row_cumsum_kernel(float* __restrict__ cum, int rows, int cols)
 {
     __shared__ float tile[32][33];
@@ -865,11 +865,22 @@ __global__ void compat_row_cumsum_kernel(float* __restrict__ cum, int rows, int 
                 next[i] = (rr < rows && cc < cols) ? cum[(size_t)rr * cols + cc] : 0.f;
             }
         }
-        for (int j = 0; j < 32 && c0 + j < cols; ++j) {
-            run = __fadd_rn(run, tile[lane][j]);
-            tile[lane][j] = run;
+        // this lane's row of the tile in registers (conflict-free: bank (lane + j) % 32), the
+        // dependent adds on registers, then back
+        float v[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = tile[lane][j];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            if (c0 + j < cols) {
+                run = __fadd_rn(run, v[j]);
+                v[j] = run;
+            }
         }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) tile[lane][j] = v[j];
         __syncwarp();
+#pragma unroll
         for (int i = 0; i < 32; ++i) {
             const int rr = r0 + i, cc = c0 + lane;
             if (rr < rows && cc < cols) cum[(size_t)rr * cols + cc] = tile[i][lane];
