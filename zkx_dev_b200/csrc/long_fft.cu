@@ -154,18 +154,25 @@ __device__ __forceinline__ void cross_natural_scatter(const cg::cluster_group& c
 }
 
 // Twiddles of the cross-CTA passes of one CTA of the persistent kernel, the same for every
-// pulse it transforms.  Forward pass: W_N^(n2 k1) for n2 = c S + t + T j is
-// base[k1 - 1] * step[j (R - 1) + k1 - 1] with base = W_N^((c S + t) k1) per thread and
-// step = W_N^(T j k1) shared.  Inverse pass of CTA k1: W_N^(-m k1) for m = t + T r is
+// pulse it transforms.  Clusters of two take the forward pass on position pairs (PAIRED:
+// 128-bit loads and remote stores; measured 1.7-2% faster at 32768 points, 4-5% slower at
+// 65536 with clusters of four, which keep single positions).  Forward pass, position
+// n2 = c S + P (t + T j) (+1 for the pair's second, P = 2 when PAIRED, else 1):
+// W_N^(n2 k1) = base[k1 - 1] (base1 for the second) * step[j (R - 1) + k1 - 1] with
+// base = W_N^((c S + P t) k1), base1 = W_N^((c S + P t + 1) k1) per thread and
+// step = W_N^(P T j k1) shared.  Inverse pass of CTA k1: W_N^(-m k1) for m = t + T r is
 // ibase * istep[r] with ibase = W_N^(-t k1), istep = W_N^(-T r k1).  One complex product
 // replaces a table load per value (the product differs from the table value by about one
 // unit in the last place).
 template <int R>
 struct CrossTwiddles {
+    static constexpr bool PAIRED = R == 2;
+    static constexpr int P = PAIRED ? 2 : 1;
     static constexpr int PER = kM / R / kT;
-    static constexpr int STEP = PER * (R - 1);   // forward steps
-    static constexpr int WORDS = STEP + kE;       // shared words (forward + inverse steps)
+    static constexpr int STEP = PER / P * (R - 1);   // forward steps
+    static constexpr int WORDS = STEP + kE;           // shared words (forward + inverse steps)
     float2 base[R - 1];
+    float2 base1[R - 1];
     float2 ibase;
 };
 
@@ -177,47 +184,78 @@ __device__ __forceinline__ void cross_twiddles_init(CrossTwiddles<R>& c, float2*
     using CT = CrossTwiddles<R>;
     for (int i = t; i < CT::STEP; i += kT) {
         const int j = i / (R - 1), k = i - j * (R - 1) + 1;
-        steps[i] = long_twiddle<R, -1>(tw, kT * j * k);
+        steps[i] = long_twiddle<R, -1>(tw, CT::P * kT * j * k);
     }
     for (int r = t; r < kE; r += kT) steps[CT::STEP + r] = long_twiddle<R, 1>(tw, kT * r * k1);
 #pragma unroll
-    for (int k = 1; k < R; ++k) c.base[k - 1] = long_twiddle<R, -1>(tw, (k1 * (kM / R) + t) * k);
+    for (int k = 1; k < R; ++k) {
+        c.base[k - 1] = long_twiddle<R, -1>(tw, (k1 * (kM / R) + CT::P * t) * k);
+        c.base1[k - 1] = long_twiddle<R, -1>(tw, (k1 * (kM / R) + CT::P * t + 1) * k);
+    }
     c.ibase = long_twiddle<R, 1>(tw, t * k1);
 }
 
-// cross_dif_scatter (forward, DIR -1) with the twiddles of cross_twiddles_init.
-template <int R, class Load>
-__device__ __forceinline__ void cross_dif_scatter_tw(const cg::cluster_group& cl, float2* sm, int c, int t,
-                                                     const CrossTwiddles<R>& ct, const float2* steps, Load load)
+__device__ __forceinline__ void store_cluster2(uint32_t address, float2 a, float2 b)
 {
+    asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(address), "f"(a.x), "f"(a.y),
+                 "f"(b.x), "f"(b.y)
+                 : "memory");
+}
+
+// cross_dif_scatter (forward, DIR -1) with the twiddles of cross_twiddles_init.  load2(e)
+// returns elements e and e + 1 as one float4 (only .x, .y used for single positions).
+template <int R, class Load2>
+__device__ __forceinline__ void cross_dif_scatter_tw(const cg::cluster_group& cl, float2* sm, int c, int t,
+                                                     const CrossTwiddles<R>& ct, const float2* steps, Load2 load2)
+{
+    using CT = CrossTwiddles<R>;
     constexpr int S = kM / R, PER = S / kT;
+    static_assert(PER % CT::P == 0, "position pairs");
     uint32_t dst[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) dst[k] = cluster_address(sm, k);
     cl.sync();  // every CTA of the cluster is running before its shared memory is written
 #pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        const int n2 = c * S + t + kT * j;
-        float2 a[R];
+    for (int j = 0; j < PER / CT::P; ++j) {
+        const int n2 = c * S + CT::P * (t + kT * j);
+        float2 a[R], b[R];
 #pragma unroll
-        for (int n1 = 0; n1 < R; ++n1) a[n1] = load(n1 * kM + n2);
+        for (int n1 = 0; n1 < R; ++n1) {
+            const float4 q = load2(n1 * kM + n2);
+            a[n1] = make_float2(q.x, q.y);
+            b[n1] = make_float2(q.z, q.w);
+        }
         dft<R, -1>(a);
-        store_cluster(dst[0] + 8u * n2, a[0]);
+        if constexpr (CT::PAIRED) {
+            dft<R, -1>(b);
+            store_cluster2(dst[0] + 8u * n2, a[0], b[0]);
 #pragma unroll
-        for (int k1 = 1; k1 < R; ++k1)
-            store_cluster(dst[k1] + 8u * n2, cmul(a[k1], cmul(ct.base[k1 - 1], steps[j * (R - 1) + k1 - 1])));
+            for (int k1 = 1; k1 < R; ++k1) {
+                const float2 st = steps[j * (R - 1) + k1 - 1];
+                store_cluster2(dst[k1] + 8u * n2, cmul(a[k1], cmul(ct.base[k1 - 1], st)),
+                               cmul(b[k1], cmul(ct.base1[k1 - 1], st)));
+            }
+        } else {
+            store_cluster(dst[0] + 8u * n2, a[0]);
+#pragma unroll
+            for (int k1 = 1; k1 < R; ++k1)
+                store_cluster(dst[k1] + 8u * n2, cmul(a[k1], cmul(ct.base[k1 - 1], steps[j * (R - 1) + k1 - 1])));
+        }
     }
     cl.sync();  // all of this CTA's b values have arrived
 }
 
-// cross_dit_gather (inverse, DIR +1, unscaled) with the twiddles of cross_twiddles_init.
+// cross_dit_gather (inverse, DIR +1, unscaled) with the twiddles of cross_twiddles_init; with
+// PAIRED the final butterflies take position pairs (128-bit shared loads, and 128-bit stores
+// when yr is 16-byte aligned).
 template <int R>
 __device__ __forceinline__ void cross_dit_gather_tw(const cg::cluster_group& cl, const float2 (&v)[kE], float2* sm,
                                                     int k1, int t, const CrossTwiddles<R>& ct, const float2* steps,
                                                     float2* yr)
 {
+    using CT = CrossTwiddles<R>;
     constexpr int S = kM / R, PER = S / kT;
-    const float2* istep = steps + CrossTwiddles<R>::STEP;
+    const float2* istep = steps + CT::STEP;
     uint32_t dst[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) dst[k] = cluster_address(sm, k);
@@ -228,15 +266,42 @@ __device__ __forceinline__ void cross_dit_gather_tw(const cg::cluster_group& cl,
         store_cluster(dst[r / PER] + 8u * (k1 * S + t + kT * (r % PER)), zv);
     }
     cl.sync();
+    if constexpr (CT::PAIRED) {
+        const bool pairs = (reinterpret_cast<uintptr_t>(yr) & 15) == 0;
 #pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        const int mm = t + kT * j;
-        float2 a[R];
+        for (int j = 0; j < PER / 2; ++j) {
+            const int mm = 2 * (t + kT * j);
+            float2 a[R], b[R];
 #pragma unroll
-        for (int k = 0; k < R; ++k) a[k] = sm[k * S + mm];
-        dft<R, 1>(a);
+            for (int k = 0; k < R; ++k) {
+                const float4 q = *reinterpret_cast<const float4*>(&sm[k * S + mm]);
+                a[k] = make_float2(q.x, q.y);
+                b[k] = make_float2(q.z, q.w);
+            }
+            dft<R, 1>(a);
+            dft<R, 1>(b);
 #pragma unroll
-        for (int c = 0; c < R; ++c) yr[(size_t)c * kM + k1 * S + mm] = a[c];
+            for (int c = 0; c < R; ++c) {
+                float2* o = yr + (size_t)c * kM + k1 * S + mm;
+                if (pairs) {
+                    *reinterpret_cast<float4*>(o) = make_float4(a[c].x, a[c].y, b[c].x, b[c].y);
+                } else {
+                    o[0] = a[c];
+                    o[1] = b[c];
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const int mm = t + kT * j;
+            float2 a[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) a[k] = sm[k * S + mm];
+            dft<R, 1>(a);
+#pragma unroll
+            for (int c = 0; c < R; ++c) yr[(size_t)c * kM + k1 * S + mm] = a[c];
+        }
     }
 }
 
@@ -408,8 +473,18 @@ long_compression_local_kernel(const Src src, int pulses, int samples, const floa
                 bulk_prefetch_l2(nx + lo, (uint32_t)(hi - lo) * (uint32_t)sizeof(float2));
         }
         const float2* xr = src.row(pulse);
-        cross_dif_scatter_tw<R>(cl, sm, k1, t, ct, steps,
-                                [&](int e) { return e < avail ? __ldcs(&xr[e]) : make_float2(0.f, 0.f); });
+        const bool aligned = (reinterpret_cast<uintptr_t>(xr) & 15) == 0;
+        cross_dif_scatter_tw<R>(cl, sm, k1, t, ct, steps, [&](int e) {
+            if constexpr (CrossTwiddles<R>::PAIRED) {
+                if (aligned && e + 1 < avail) return __ldcs(reinterpret_cast<const float4*>(xr + e));
+                const float2 u = e < avail ? __ldcs(&xr[e]) : make_float2(0.f, 0.f);
+                const float2 w = e + 1 < avail ? __ldcs(&xr[e + 1]) : make_float2(0.f, 0.f);
+                return make_float4(u.x, u.y, w.x, w.y);
+            } else {
+                const float2 u = e < avail ? __ldcs(&xr[e]) : make_float2(0.f, 0.f);
+                return make_float4(u.x, u.y, 0.f, 0.f);
+            }
+        });
         float2 v[kE];
         take_own(v, sm, t);
         local_fft_forward<LP>(v, sm, t, twiddle, tab);
