@@ -175,7 +175,9 @@ class ChainGraph:
 
 
 class WorkList:
-    """The chain over CPIs of mixed shapes, one launch per stage (zkx_rd_worklist_*).
+    """The chain over CPIs of mixed shapes, one launch per stage and resource class
+    (zkx_rd_worklist_*; plans whose stages the work-list kernels do not cover run those
+    stages on their own kernels).
 
     ``items`` is a sequence of ``(chain, x, outputs)``: a RangeDopplerChain (its plan gives
     the CPI's shape and parameters), the device input CPI and a dict with device
